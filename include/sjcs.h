@@ -1,0 +1,223 @@
+/*
+ * sjcs.h -- C ABI of the B200 (sm_100a) spatial-join-count-over-shells hot path.
+ *
+ * The reference program (astr_rcount) builds one STR tree per particle file and
+ * then, for every halo, counts the particles that fall into each of n radial
+ * shells under a periodic [0,1000)^3 box.  Its index layer is a per-halo C API:
+ *
+ *   constructArraySTR / insertDataArraySTR / makeTreeWithSameThreadPoolArraySTR
+ *       include/objects/ArraySTR/ArraySTR.h:52-56
+ *   multiRangeCountWithPriodicBoundArraySTR / multiRangeCountArraySTR
+ *       include/objects/ArraySTR/MultiRangeCount.h:10-11
+ *   MultiRangeCountContext {nrads, central, radiuses (squared, ascending), counts}
+ *       include/objects/RTree/MultiRangeCountContext.h:7-18
+ *   destructArraySTR  include/objects/ArraySTR/ArraySTR.h:53
+ *
+ * and the driver calls it once per halo from a thread pool
+ * (threadJoin, src/astr_rcount/main.c:795-826).  A per-halo call cannot feed a
+ * GPU, so this ABI keeps the same seam -- build an index over one particle
+ * file, count shells for a set of halos against it, accumulate counts across
+ * files, destroy the index -- but batched over all halos at once.
+ *
+ * Conventions
+ *  - Every entry point returns an int status (SJCS_OK == 0).  On failure,
+ *    sjcs_last_error() returns a message for the calling thread.
+ *  - Objects are opaque handles owned by the caller.  A context owns one GPU
+ *    and its streams; indexes and queries belong to the context that made them.
+ *  - Counts follow the reference: per halo, per shell, unsigned 64-bit on the
+ *    host, INCREMENTED (never cleared) by each particle file's pass.  A particle
+ *    lands in the first shell i with dist < r2[i] (dist = squared distance in
+ *    fp32, (dx*dx + dy*dy) + dz*dz, no FMA) after passing the inclusive query
+ *    box test; periodic images follow the reference's out-of-bound rule.
+ *  - Pointers named d_* are device pointers; all others are host pointers.
+ *  - No entry point falls back to a CPU implementation: without a usable GPU
+ *    they fail with SJCS_ERR_CUDA.
+ */
+#ifndef SJCS_H
+#define SJCS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define SJCS_OK            0
+#define SJCS_ERR_INVALID   1  /* bad argument (null pointer, bad size, bad radius table) */
+#define SJCS_ERR_CUDA      2  /* CUDA runtime error or no usable device */
+#define SJCS_ERR_NOMEM     3  /* device or pinned-host allocation failed */
+#define SJCS_ERR_STATE     4  /* object used with another context, or after destroy */
+#define SJCS_ERR_TIMEOUT   5  /* a bounded device-side wait gave up (error flag set) */
+
+/* index kinds */
+#define SJCS_INDEX_GRID     0 /* uniform cell grid: particles radix-sorted by cell, cell-offset table */
+#define SJCS_INDEX_LEARNED  1 /* Morton-sorted particles + two-level piecewise-linear rank model */
+
+/* query flags */
+#define SJCS_QUERY_PERIODIC     0x1 /* periodic images, as multiRangeCountWithPriodicBoundArraySTR */
+#define SJCS_QUERY_NONPERIODIC  0x0 /* single image, as multiRangeCountArraySTR (MultiRangeCount.c:75-83) */
+
+typedef struct sjcs_ctx   sjcs_ctx;   /* one GPU: streams, scratch, tuning cache */
+typedef struct sjcs_index sjcs_index; /* device-resident index over one particle file */
+typedef struct sjcs_query sjcs_query; /* device-resident halos + radius table + u32 count accumulators */
+
+/* Build options.  Zero-initialised options select an automatic grid for the
+ * plain index (sized from n and radius_hint). */
+typedef struct sjcs_index_opts {
+    int      kind;         /* SJCS_INDEX_GRID or SJCS_INDEX_LEARNED */
+    float    radius_hint;  /* largest search radius expected (sqrt of r2[nrads-1]); 0 = unknown */
+    uint32_t grid[3];      /* cells per axis (x, y, z) for SJCS_INDEX_GRID; 0 = automatic */
+    uint32_t reserved[4];  /* must be zero */
+} sjcs_index_opts;
+
+/* Timing from CUDA events on the stream that ran the work (milliseconds; 0
+ * where not applicable).  For an index: its copy and build.  For a query: the
+ * count kernels of every sjcs_query_count since creation or the last
+ * sjcs_query_reset (count_ms is their sum, count_calls their number) and the
+ * last read-back. */
+typedef struct sjcs_timing {
+    float h2d_ms;         /* host-to-device copy inside the call */
+    float build_ms;       /* index build kernels (key, radix sort, gather, offsets) */
+    float count_ms;       /* shell-count kernel(s) */
+    float d2h_ms;         /* device-to-host read-back (widening kernel + copy) */
+    uint32_t count_calls; /* number of sjcs_query_count calls summed in count_ms */
+} sjcs_timing;
+
+/* ---- errors / version ---------------------------------------------------- */
+
+/* Message for the last failing call on this thread ("" if none).  Replaces the
+ * reference's stderr prints before NULL returns (e.g. src/Gadget/BufHalo.c:85-98). */
+const char *sjcs_last_error(void);
+/* Library version string. */
+const char *sjcs_version(void);
+
+/* ---- context ------------------------------------------------------------- */
+
+/* Open a context on CUDA device `device`.  The reference's analogue is the
+ * SameThreadPool the driver builds before the file loop
+ * (src/astr_rcount/main.c:245, constructSameThreadPool). */
+int sjcs_ctx_create(int device, sjcs_ctx **out);
+/* Wait for all work of the context and release it (main.c:263,
+ * destructSameThreadPool). */
+int sjcs_ctx_destroy(sjcs_ctx *ctx);
+/* Block until every stream of the context is idle (the reference's
+ * waitCompletionSameThreadPool, src/objects/SameThreadPool/SameThreadPool.c:62-68). */
+int sjcs_ctx_sync(sjcs_ctx *ctx);
+/* Number of streaming multiprocessors of the context's device. */
+int sjcs_ctx_num_sms(const sjcs_ctx *ctx, int *out);
+/* The context's CUDA streams (cudaStream_t): which = 0 build stream (copies and
+ * index builds), 1 count stream (halo preparation, counts, read-back).  Lets a
+ * caller order its own work or timing events against the library's. */
+int sjcs_ctx_stream(const sjcs_ctx *ctx, int which, void **stream);
+/* Number of kernels this library has launched in this process so far. */
+uint64_t sjcs_launch_counter(void);
+
+/* ---- pinned host memory (for the driver's file reads) -------------------- */
+
+/* Page-locked host buffer, so that file reads land in memory the copy engines
+ * can read at full speed.  Replaces the malloc in reallocBufFloatVector3D
+ * (src/Gadget/BufVector3D.c, used by readDecodedParticles :285-308). */
+int sjcs_host_alloc(size_t bytes, void **out);
+int sjcs_host_free(void *p);
+
+/* ---- index (one particle file) ------------------------------------------- */
+
+/* Build an index over n particles given as x,y,z float triplets in HOST
+ * memory (the layout of a decoded particle file).  The copy to the device and
+ * the build run asynchronously on the context's build stream; the call returns
+ * once the work is queued and the host buffer may be reused only after
+ * sjcs_index_wait (or any later call that waits on the index).
+ * Replaces constructArraySTR + insertDataArraySTR x n +
+ * makeTreeWithSameThreadPoolArraySTR (include/objects/ArraySTR/ArraySTR.h:52-56,
+ * called from constructIndexWithSameThreadPool, src/astr_rcount/main.c:732-786).
+ * n == 0 is allowed and yields an index that matches nothing (the reference
+ * refuses to build it, src/objects/ArraySTR/Build.c:860-863). */
+int sjcs_index_build(sjcs_ctx *ctx, const float *xyz, uint64_t n,
+                     const sjcs_index_opts *opts, sjcs_index **out);
+/* Same, with the particles already in device memory (d_xyz, n*3 floats). */
+int sjcs_index_build_device(sjcs_ctx *ctx, const float *d_xyz, uint64_t n,
+                            const sjcs_index_opts *opts, sjcs_index **out);
+/* Block until the index is built. */
+int sjcs_index_wait(sjcs_index *idx);
+/* Number of particles in the index (getNumberOfDataArraySTR, ArraySTR.h:58). */
+int sjcs_index_size(const sjcs_index *idx, uint64_t *out);
+/* Cells per axis actually used by a grid index (or the Morton leaf grid of a
+ * learned index). */
+int sjcs_index_grid(const sjcs_index *idx, uint32_t out[3]);
+/* Timing of the build (valid after sjcs_index_wait). */
+int sjcs_index_timing(const sjcs_index *idx, sjcs_timing *out);
+/* Release the index after all queued work that reads it
+ * (destructArraySTR, include/objects/ArraySTR/ArraySTR.h:53). */
+int sjcs_index_destroy(sjcs_index *idx);
+
+/* ---- query (halos + shells + count accumulators) ------------------------- */
+
+/* Upload nhalos halo centres and the squared-radius table and prepare device
+ * count accumulators (zeroed).  halo_xyz points at the first halo's x; halos
+ * are `stride_bytes` apart with y,z following x (stride 24 and a pointer to
+ * Halo.point reads the reference's BufHalo array directly,
+ * include/Gadget/BufHalo.h:26-30; stride 12 reads packed triplets).
+ * r2 holds nrads squared radii as built by the driver (Logspace then r*r,
+ * src/astr_rcount/main.c:644-649); any table is accepted -- a non-decreasing,
+ * finite one takes the fast binning path, anything else the reference's
+ * first-match scan.  flags: SJCS_QUERY_PERIODIC or SJCS_QUERY_NONPERIODIC.
+ * Replaces constructMultiRangeCountContext + the per-row set-up in threadJoin
+ * (src/objects/RTree/MultiRangeCountContext.c:8-25, src/astr_rcount/main.c:816-821). */
+int sjcs_query_create(sjcs_ctx *ctx, const float *halo_xyz, size_t stride_bytes,
+                      uint64_t nhalos, const float *r2, int nrads, int flags,
+                      sjcs_query **out);
+/* Same, halos already in device memory. */
+int sjcs_query_create_device(sjcs_ctx *ctx, const float *d_halo_xyz, size_t stride_bytes,
+                             uint64_t nhalos, const float *r2, int nrads, int flags,
+                             sjcs_query **out);
+/* Count every halo of the query against one index and add the counts to the
+ * query's device accumulators (queued on the count stream after the index's
+ * build).  Replaces one file's pass of threadJoin, i.e. nhalos calls of
+ * multiRangeCountWithPriodicBoundArraySTR (include/objects/ArraySTR/MultiRangeCount.h:11)
+ * or, without SJCS_QUERY_PERIODIC, of multiRangeCountArraySTR (:10). */
+int sjcs_query_count(sjcs_ctx *ctx, sjcs_query *q, const sjcs_index *idx);
+/* Block until the last sjcs_query_count queued on q has finished (builds
+ * queued on the build stream keep running). */
+int sjcs_query_wait(sjcs_query *q);
+/* Copy the accumulated counts to host memory as uint64 [nhalos][nrads] in the
+ * order the halos were given.  accumulate != 0 adds them to `counts` (the
+ * reference's += on its calloc'd ulong_t array, src/astr_rcount/main.c:651),
+ * accumulate == 0 overwrites.  Blocks until the copy is done. */
+int sjcs_query_read_counts(sjcs_ctx *ctx, sjcs_query *q, uint64_t *counts, int accumulate);
+/* Device pointer to the query's uint32 accumulators [nhalos][nrads] in the
+ * order the halos were given (valid until sjcs_query_destroy). */
+int sjcs_query_device_counts(const sjcs_query *q, uint32_t **d_counts);
+/* Zero the accumulators and the timing history (start a new run over the
+ * same halos). */
+int sjcs_query_reset(sjcs_ctx *ctx, sjcs_query *q);
+/* Count-kernel time summed over the sjcs_query_count calls since creation or
+ * reset, and the last read-back time (blocks until those are done). */
+int sjcs_query_timing(const sjcs_query *q, sjcs_timing *out);
+int sjcs_query_destroy(sjcs_query *q);
+
+/* ---- one-shot, reference semantics --------------------------------------- */
+
+/* counts[h*nrads + i] += number of particles of idx in shell i of halo h, for
+ * the nhalos halos at halo_xyz (host, stride as above).  Synchronous.  This is
+ * threadJoin's whole loop for one file (src/astr_rcount/main.c:795-826) with
+ * the same argument meaning as MultiRangeCountContext. */
+int sjcs_multi_range_count(sjcs_ctx *ctx, const sjcs_index *idx,
+                           const float *halo_xyz, size_t stride_bytes, uint64_t nhalos,
+                           const float *r2, int nrads, int flags, uint64_t *counts);
+
+/* ---- radius schedule ----------------------------------------------------- */
+
+/* r2[i] = (float)pow(2, log2(min) + i*(log2(max)-log2(min))/(n-1)) squared in
+ * fp32, last entry (float)pow(2, log2(max)) squared -- Logspace
+ * (include/support_functions.h:18-34) followed by r[i] *= r[i]
+ * (src/astr_rcount/main.c:646-649).  min > max is swapped as the driver does
+ * (main.c:531-533).  Host-only; needs no GPU. */
+int sjcs_radius_table(double minrad, double maxrad, int nrads, float *r2);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SJCS_H */

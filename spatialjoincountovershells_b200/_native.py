@@ -1,0 +1,485 @@
+"""ctypes bindings of libsjcs.so (GPU, include/sjcs.h) and libsjcs_host.so (CPU, include/sjcs_host.h)."""
+from __future__ import annotations
+
+import ctypes
+import os
+import pathlib
+import threading
+
+import numpy as np
+
+_PKG = pathlib.Path(__file__).resolve().parent
+lib_path = _PKG / "lib" / "libsjcs.so"
+host_lib_path = _PKG / "lib" / "libsjcs_host.so"
+
+INDEX_GRID = 0
+INDEX_LEARNED = 1
+QUERY_NONPERIODIC = 0
+QUERY_PERIODIC = 1
+
+# The reference's Halo struct (include/Gadget/BufHalo.h:26-30), 24 bytes.
+HALO_DTYPE = np.dtype([("id", "<u8"), ("mass", "<f4"), ("point", "<f4", (3,))], align=False)
+assert HALO_DTYPE.itemsize == 24
+
+_c = ctypes
+_vp = _c.c_void_p
+_u64 = _c.c_uint64
+_pp = _c.POINTER(_c.c_void_p)
+
+
+class SjcsError(RuntimeError):
+    """A libsjcs / libsjcs_host call failed (code, message)."""
+
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+        self.msg = msg
+
+
+class sjcs_index_opts(_c.Structure):
+    _fields_ = [("kind", _c.c_int), ("radius_hint", _c.c_float), ("grid", _c.c_uint32 * 3),
+                ("reserved", _c.c_uint32 * 4)]
+
+
+class sjcs_timing(_c.Structure):
+    _fields_ = [("h2d_ms", _c.c_float), ("build_ms", _c.c_float), ("count_ms", _c.c_float),
+                ("d2h_ms", _c.c_float), ("count_calls", _c.c_uint32)]
+
+
+_lock = threading.Lock()
+_lib = None
+_host = None
+
+# name -> (restype, argtypes); every function declared in include/sjcs.h
+_SIGS = {
+    "sjcs_last_error": (_c.c_char_p, []),
+    "sjcs_version": (_c.c_char_p, []),
+    "sjcs_ctx_create": (_c.c_int, [_c.c_int, _pp]),
+    "sjcs_ctx_destroy": (_c.c_int, [_vp]),
+    "sjcs_ctx_sync": (_c.c_int, [_vp]),
+    "sjcs_ctx_num_sms": (_c.c_int, [_vp, _c.POINTER(_c.c_int)]),
+    "sjcs_ctx_stream": (_c.c_int, [_vp, _c.c_int, _pp]),
+    "sjcs_launch_counter": (_c.c_uint64, []),
+    "sjcs_host_alloc": (_c.c_int, [_c.c_size_t, _pp]),
+    "sjcs_host_free": (_c.c_int, [_vp]),
+    "sjcs_index_build": (_c.c_int, [_vp, _vp, _u64, _c.POINTER(sjcs_index_opts), _pp]),
+    "sjcs_index_build_device": (_c.c_int, [_vp, _vp, _u64, _c.POINTER(sjcs_index_opts), _pp]),
+    "sjcs_index_wait": (_c.c_int, [_vp]),
+    "sjcs_index_size": (_c.c_int, [_vp, _c.POINTER(_u64)]),
+    "sjcs_index_grid": (_c.c_int, [_vp, _c.POINTER(_c.c_uint32)]),
+    "sjcs_index_timing": (_c.c_int, [_vp, _c.POINTER(sjcs_timing)]),
+    "sjcs_index_destroy": (_c.c_int, [_vp]),
+    "sjcs_query_create": (_c.c_int, [_vp, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _pp]),
+    "sjcs_query_create_device": (_c.c_int, [_vp, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _pp]),
+    "sjcs_query_count": (_c.c_int, [_vp, _vp, _vp]),
+    "sjcs_query_wait": (_c.c_int, [_vp]),
+    "sjcs_query_read_counts": (_c.c_int, [_vp, _vp, _vp, _c.c_int]),
+    "sjcs_query_device_counts": (_c.c_int, [_vp, _pp]),
+    "sjcs_query_reset": (_c.c_int, [_vp, _vp]),
+    "sjcs_query_timing": (_c.c_int, [_vp, _c.POINTER(sjcs_timing)]),
+    "sjcs_query_destroy": (_c.c_int, [_vp]),
+    "sjcs_multi_range_count": (_c.c_int, [_vp, _vp, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _vp]),
+    "sjcs_radius_table": (_c.c_int, [_c.c_double, _c.c_double, _c.c_int, _vp]),
+}
+
+_HOST_SIGS = {
+    "sjcs_particle_file_count": (_c.c_int, [_c.c_char_p, _c.POINTER(_u64)]),
+    "sjcs_read_particles": (_c.c_int, [_c.c_char_p, _vp, _u64, _c.POINTER(_u64)]),
+    "sjcs_read_halos": (_c.c_int, [_c.c_char_p, _pp, _c.POINTER(_u64), _c.c_int]),
+    "sjcs_read_and_filter_halos": (_c.c_int, [_c.c_char_p, _c.c_char_p, _pp, _c.POINTER(_u64)]),
+    "sjcs_host_free_halos": (None, [_vp]),
+    "sjcs_host_last_error": (_c.c_char_p, []),
+    "sjcs_write_result": (_c.c_int, [_c.c_char_p, _vp, _u64, _vp, _c.c_int, _vp, _c.c_int]),
+    "sjcs_host_radius_table": (_c.c_int, [_c.c_double, _c.c_double, _c.c_int, _vp]),
+    "sjcs_mt_seed": (None, [_vp, _c.c_uint32]),
+    "sjcs_mt_u32": (_c.c_uint32, [_vp]),
+    "sjcs_mt_real1": (_c.c_double, [_vp]),
+    "sjcs_gen_uniform_particles": (_c.c_int, [_c.c_uint32, _u64, _u64, _vp]),
+    "sjcs_gen_uniform_halo_file": (_c.c_int, [_c.c_char_p, _c.c_uint32, _u64, _u64]),
+    "sjcs_gen_uniform_halos": (_c.c_int, [_c.c_uint32, _u64, _u64, _vp, _c.c_int]),
+    "sjcs_gen_face_halos": (_c.c_int, [_c.c_uint32, _u64, _u64, _c.c_float, _vp]),
+    "sjcs_gen_clustered_particles": (_c.c_int, [_c.c_uint32, _u64, _c.c_uint32, _c.c_double, _c.c_double,
+                                                 _c.c_double, _c.c_double, _c.c_uint32, _vp]),
+    "sjcs_gen_clustered_halos": (_c.c_int, [_c.c_uint32, _u64, _u64, _c.c_uint32, _c.c_double, _c.c_double,
+                                             _c.c_double, _c.c_double, _c.c_double, _c.c_uint32, _vp]),
+    "sjcs_write_halo_file": (_c.c_int, [_c.c_char_p, _vp, _u64]),
+    "sjcs_write_particle_file": (_c.c_int, [_c.c_char_p, _vp, _u64]),
+}
+
+
+def _bind(handle, sigs):
+    for name, (res, args) in sigs.items():
+        f = getattr(handle, name)
+        f.restype = res
+        f.argtypes = args
+    return handle
+
+
+def lib():
+    """libsjcs.so (GPU path).  Raises if it has not been built: there is no CPU fallback."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not lib_path.exists():
+                raise SjcsError(2, f"{lib_path} is missing; build it with "
+                                   "`python -m spatialjoincountovershells_b200.build`")
+            _lib = _bind(ctypes.CDLL(str(lib_path)), _SIGS)
+        return _lib
+
+
+def host_lib():
+    global _host
+    with _lock:
+        if _host is None:
+            if not host_lib_path.exists():
+                raise SjcsError(2, f"{host_lib_path} is missing; build it with "
+                                   "`python -m spatialjoincountovershells_b200.build`")
+            _host = _bind(ctypes.CDLL(str(host_lib_path)), _HOST_SIGS)
+        return _host
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise SjcsError(rc, lib().sjcs_last_error().decode(errors="replace"))
+
+
+def _hcheck(rc: int) -> None:
+    if rc != 0:
+        raise SjcsError(rc, host_lib().sjcs_host_last_error().decode(errors="replace"))
+
+
+def _ptr(a) -> int:
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    if hasattr(a, "data_ptr"):
+        return a.data_ptr()
+    return int(a)
+
+
+def _is_cuda(a) -> bool:
+    return hasattr(a, "is_cuda") and bool(a.is_cuda)
+
+
+def _as_f32_xyz(a) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if a.ndim != 2 or a.shape[1] != 3:
+        a = a.reshape(-1, 3)
+    return a
+
+
+# ---------------------------------------------------------------------------
+# GPU objects
+# ---------------------------------------------------------------------------
+
+class Context:
+    """One GPU (sjcs_ctx): a build stream and a count stream."""
+
+    def __init__(self, device: int = 0):
+        h = _vp()
+        _check(lib().sjcs_ctx_create(int(device), _c.byref(h)))
+        self._h = h
+        self.device = device
+
+    @property
+    def handle(self):
+        return self._h
+
+    @property
+    def num_sms(self) -> int:
+        v = _c.c_int()
+        _check(lib().sjcs_ctx_num_sms(self._h, _c.byref(v)))
+        return v.value
+
+    def sync(self) -> None:
+        _check(lib().sjcs_ctx_sync(self._h))
+
+    def stream(self, which: int) -> int:
+        """cudaStream_t of the build (0) or count (1) stream, as an integer."""
+        p = _vp()
+        _check(lib().sjcs_ctx_stream(self._h, int(which), _c.byref(p)))
+        return p.value or 0
+
+    def close(self) -> None:
+        if self._h:
+            _check(lib().sjcs_ctx_destroy(self._h))
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def build_index(self, xyz, radius_hint: float = 0.0, grid=None, kind: int = INDEX_GRID) -> "Index":
+        """Index over particles: host array (n,3) float32, or a CUDA tensor (device path)."""
+        opts = sjcs_index_opts()
+        opts.kind = kind
+        opts.radius_hint = float(radius_hint)
+        if grid is not None:
+            for a in range(3):
+                opts.grid[a] = int(grid[a])
+        h = _vp()
+        if _is_cuda(xyz):
+            n = xyz.numel() // 3
+            _check(lib().sjcs_index_build_device(self._h, _vp(xyz.data_ptr()), n, _c.byref(opts), _c.byref(h)))
+            keep = xyz
+        else:
+            arr = _as_f32_xyz(xyz)
+            n = arr.shape[0]
+            _check(lib().sjcs_index_build(self._h, _vp(arr.ctypes.data if n else 0), n, _c.byref(opts),
+                                          _c.byref(h)))
+            keep = arr
+        return Index(self, h, keep)
+
+    def query(self, halos, r2, periodic: bool = True) -> "Query":
+        """Halo set + squared-radius table.  halos: (n,3) float32, a HALO_DTYPE array
+        (its .point field is read in place with stride 24), or a CUDA tensor."""
+        r2 = np.ascontiguousarray(r2, dtype=np.float32)
+        flags = QUERY_PERIODIC if periodic else QUERY_NONPERIODIC
+        h = _vp()
+        if _is_cuda(halos):
+            stride = 4 * (halos.shape[-1] if halos.dim() == 2 else 3)
+            n = halos.shape[0] if halos.dim() == 2 else halos.numel() // 3
+            _check(lib().sjcs_query_create_device(self._h, _vp(halos.data_ptr()), stride, n,
+                                                  _vp(r2.ctypes.data), len(r2), flags, _c.byref(h)))
+            keep = halos
+        else:
+            if isinstance(halos, np.ndarray) and halos.dtype == HALO_DTYPE:
+                arr = np.ascontiguousarray(halos)
+                base = arr.ctypes.data + HALO_DTYPE.fields["point"][1]
+                stride = HALO_DTYPE.itemsize
+            else:
+                arr = _as_f32_xyz(halos)
+                base = arr.ctypes.data
+                stride = 12
+            n = arr.shape[0]
+            _check(lib().sjcs_query_create(self._h, _vp(base if n else 0), stride, n, _vp(r2.ctypes.data),
+                                           len(r2), flags, _c.byref(h)))
+            keep = arr
+        return Query(self, h, n, len(r2), keep)
+
+
+class Index:
+    def __init__(self, ctx: Context, h, keep):
+        self.ctx = ctx
+        self._h = h
+        self._keep = keep  # host buffer must live until the build is done
+
+    def wait(self) -> "Index":
+        _check(lib().sjcs_index_wait(self._h))
+        self._keep = None
+        return self
+
+    @property
+    def size(self) -> int:
+        v = _u64()
+        _check(lib().sjcs_index_size(self._h, _c.byref(v)))
+        return v.value
+
+    @property
+    def grid(self):
+        g = (_c.c_uint32 * 3)()
+        _check(lib().sjcs_index_grid(self._h, g))
+        return tuple(g)
+
+    def timing(self) -> dict:
+        t = sjcs_timing()
+        _check(lib().sjcs_index_timing(self._h, _c.byref(t)))
+        return {"h2d_ms": t.h2d_ms, "build_ms": t.build_ms}
+
+    def destroy(self) -> None:
+        if self._h:
+            _check(lib().sjcs_index_destroy(self._h))
+            self._h = None
+            self._keep = None
+
+    def __del__(self):
+        try:
+            if self._h and self.ctx._h:
+                lib().sjcs_index_destroy(self._h)
+        except Exception:
+            pass
+
+
+class Query:
+    def __init__(self, ctx: Context, h, nhalos: int, nrads: int, keep):
+        self.ctx = ctx
+        self._h = h
+        self.nhalos = nhalos
+        self.nrads = nrads
+        self._keep = keep
+
+    def count(self, index: Index) -> "Query":
+        _check(lib().sjcs_query_count(self.ctx._h, self._h, index._h))
+        return self
+
+    def wait(self) -> "Query":
+        _check(lib().sjcs_query_wait(self._h))
+        return self
+
+    def read_counts(self, out: np.ndarray | None = None, accumulate: bool = False) -> np.ndarray:
+        if out is None:
+            out = np.zeros((self.nhalos, self.nrads), dtype=np.uint64)
+        elif out.dtype != np.uint64 or not out.flags.c_contiguous or out.size != self.nhalos * self.nrads:
+            raise ValueError("out must be a C-contiguous uint64 array of nhalos*nrads elements")
+        _check(lib().sjcs_query_read_counts(self.ctx._h, self._h, _vp(_ptr(out)), 1 if accumulate else 0))
+        return out
+
+    def read_counts_into(self, ptr: int, accumulate: bool = False) -> None:
+        """Read into caller memory given by address (e.g. a pinned torch tensor)."""
+        _check(lib().sjcs_query_read_counts(self.ctx._h, self._h, _vp(ptr), 1 if accumulate else 0))
+
+    @property
+    def device_counts_ptr(self) -> int:
+        p = _vp()
+        _check(lib().sjcs_query_device_counts(self._h, _c.byref(p)))
+        return p.value or 0
+
+    def reset(self) -> None:
+        _check(lib().sjcs_query_reset(self.ctx._h, self._h))
+
+    def timing(self) -> dict:
+        t = sjcs_timing()
+        _check(lib().sjcs_query_timing(self._h, _c.byref(t)))
+        return {"count_ms": t.count_ms, "count_calls": t.count_calls, "d2h_ms": t.d2h_ms}
+
+    def destroy(self) -> None:
+        if self._h:
+            _check(lib().sjcs_query_destroy(self._h))
+            self._h = None
+
+    def __del__(self):
+        try:
+            if self._h and self.ctx._h:
+                lib().sjcs_query_destroy(self._h)
+        except Exception:
+            pass
+
+
+def launch_counter() -> int:
+    """Kernels launched by libsjcs.so in this process so far."""
+    return int(lib().sjcs_launch_counter())
+
+
+def multi_range_count_with_periodic_bound(ctx: Context, index: Index, halos, r2, counts: np.ndarray,
+                                          periodic: bool = True) -> np.ndarray:
+    """counts (uint64 [nhalos, nrads]) += shell counts of `halos` against `index`
+    (one file's pass of threadJoin: multiRangeCountWithPriodicBoundArraySTR per halo)."""
+    r2 = np.ascontiguousarray(r2, dtype=np.float32)
+    if isinstance(halos, np.ndarray) and halos.dtype == HALO_DTYPE:
+        arr = np.ascontiguousarray(halos)
+        base, stride = arr.ctypes.data + HALO_DTYPE.fields["point"][1], 24
+    else:
+        arr = _as_f32_xyz(halos)
+        base, stride = arr.ctypes.data, 12
+    n = arr.shape[0]
+    if counts.dtype != np.uint64 or not counts.flags.c_contiguous or counts.size != n * len(r2):
+        raise ValueError("counts must be a C-contiguous uint64 array of nhalos*nrads elements")
+    _check(lib().sjcs_multi_range_count(ctx._h, index._h, _vp(base if n else 0), stride, n, _vp(r2.ctypes.data),
+                                        len(r2), QUERY_PERIODIC if periodic else QUERY_NONPERIODIC,
+                                        _vp(counts.ctypes.data)))
+    return counts
+
+
+# ---------------------------------------------------------------------------
+# host formats and generators (CPU only)
+# ---------------------------------------------------------------------------
+
+def radius_table(minrad: float, maxrad: float, nrads: int) -> np.ndarray:
+    """Squared radii as the reference driver builds them (Logspace then r*r in fp32)."""
+    out = np.zeros(nrads, dtype=np.float32)
+    _hcheck(host_lib().sjcs_host_radius_table(float(minrad), float(maxrad), int(nrads), _vp(out.ctypes.data)))
+    return out
+
+
+def read_particles(path) -> np.ndarray:
+    n = _u64()
+    _hcheck(host_lib().sjcs_particle_file_count(os.fsencode(path), _c.byref(n)))
+    out = np.empty((n.value, 3), dtype=np.float32)
+    got = _u64()
+    _hcheck(host_lib().sjcs_read_particles(os.fsencode(path), _vp(out.ctypes.data), n.value, _c.byref(got)))
+    return out[: got.value]
+
+
+def _take_halos(p, n: int) -> np.ndarray:
+    try:
+        if n == 0:
+            return np.zeros(0, dtype=HALO_DTYPE)
+        buf = (_c.c_uint8 * (n * 24)).from_address(p.value)
+        return np.frombuffer(buf, dtype=HALO_DTYPE).copy()
+    finally:
+        host_lib().sjcs_host_free_halos(p)
+
+
+def read_halos(path, filter_path=None, nthreads: int = 0) -> np.ndarray:
+    p = _vp()
+    n = _u64()
+    if filter_path is None:
+        _hcheck(host_lib().sjcs_read_halos(os.fsencode(path), _c.byref(p), _c.byref(n), int(nthreads)))
+    else:
+        _hcheck(host_lib().sjcs_read_and_filter_halos(os.fsencode(path), os.fsencode(filter_path), _c.byref(p),
+                                                      _c.byref(n)))
+    return _take_halos(p, n.value)
+
+
+def write_result(path, halos: np.ndarray, r2, counts: np.ndarray, nthreads: int = 0) -> None:
+    r2 = np.ascontiguousarray(r2, dtype=np.float32)
+    halos = np.ascontiguousarray(halos, dtype=HALO_DTYPE)
+    counts = np.ascontiguousarray(counts, dtype=np.uint64)
+    _hcheck(host_lib().sjcs_write_result(None if path is None else os.fsencode(path), _vp(halos.ctypes.data),
+                                         len(halos), _vp(r2.ctypes.data), len(r2), _vp(counts.ctypes.data),
+                                         int(nthreads)))
+
+
+def gen_uniform_particles(seed: int, nfiles: int, n: int) -> np.ndarray:
+    out = np.empty((nfiles * n, 3), dtype=np.float32)
+    _hcheck(host_lib().sjcs_gen_uniform_particles(seed, nfiles, n, _vp(out.ctypes.data)))
+    return out
+
+
+def gen_uniform_halo_file(path, seed: int, n: int, id0: int = 0) -> None:
+    _hcheck(host_lib().sjcs_gen_uniform_halo_file(os.fsencode(path), seed, n, id0))
+
+
+def gen_uniform_halos(seed: int, n: int, id0: int = 0, nthreads: int = 0) -> np.ndarray:
+    out = np.zeros(n, dtype=HALO_DTYPE)
+    _hcheck(host_lib().sjcs_gen_uniform_halos(seed, n, id0, _vp(out.ctypes.data), nthreads))
+    return out
+
+
+def gen_face_halos(seed: int, n: int, id0: int = 0, margin: float = 5.0) -> np.ndarray:
+    out = np.zeros(n, dtype=HALO_DTYPE)
+    _hcheck(host_lib().sjcs_gen_face_halos(seed, n, id0, margin, _vp(out.ctypes.data)))
+    return out
+
+
+# Clustered workload: 1e4 clumps, sigma log-uniform [2, 20], weights lognormal(0, 1.5), 60% clumped.
+CLUSTER_DEFAULTS = dict(nclumps=10000, sig_lo=2.0, sig_hi=20.0, wsig=1.5)
+
+
+def gen_clustered_particles(seed: int, n: int, frac_clumped: float = 0.6, clump_seed: int = 31,
+                            **kw) -> np.ndarray:
+    p = {**CLUSTER_DEFAULTS, **kw}
+    out = np.empty((n, 3), dtype=np.float32)
+    _hcheck(host_lib().sjcs_gen_clustered_particles(seed, n, p["nclumps"], p["sig_lo"], p["sig_hi"], p["wsig"],
+                                                    frac_clumped, clump_seed, _vp(out.ctypes.data)))
+    return out
+
+
+def gen_clustered_halos(seed: int, n: int, id0: int = 0, frac_at_clumps: float = 0.7, jitter: float = 1.0,
+                        clump_seed: int = 31, **kw) -> np.ndarray:
+    p = {**CLUSTER_DEFAULTS, **kw}
+    out = np.zeros(n, dtype=HALO_DTYPE)
+    _hcheck(host_lib().sjcs_gen_clustered_halos(seed, n, id0, p["nclumps"], p["sig_lo"], p["sig_hi"], p["wsig"],
+                                                frac_at_clumps, jitter, clump_seed, _vp(out.ctypes.data)))
+    return out
+
+
+def write_halo_file(path, halos: np.ndarray) -> None:
+    halos = np.ascontiguousarray(halos, dtype=HALO_DTYPE)
+    _hcheck(host_lib().sjcs_write_halo_file(os.fsencode(path), _vp(halos.ctypes.data), len(halos)))
+
+
+def write_particle_file(path, xyz) -> None:
+    arr = _as_f32_xyz(xyz)
+    _hcheck(host_lib().sjcs_write_particle_file(os.fsencode(path), _vp(arr.ctypes.data), arr.shape[0]))

@@ -1,0 +1,197 @@
+// Plain (grid) index build for one particle file.
+//
+// Replaces the STR bulk load of the reference (MakeTreeWithSameThreadPoolArraySTR,
+// src/objects/ArraySTR/Build.c:845-963: per level, LSD radix sorts on the
+// y, x, z centres, gather, pack 10 children per parent MBR).  The counts the
+// reference produces do not depend on the tree shape -- a leaf is reached iff
+// its point lies inside the query box, because every parent MBR is the exact
+// hull of its children (adjustMbrArraySTRNode, src/objects/ArraySTR/Node.c:10-58)
+// -- so any index that returns a superset of the in-box points gives the same
+// counts.  Here the index is a uniform cell grid:
+//   pass 0   key = cell of (x,y,z), computed from the AoS input on the fly
+//   passes   stable LSD radix sort of (key, particle id), 8 bits per pass
+//   last     the final scatter gathers x,y,z into sorted SoA arrays
+//   offsets  cell_start[c] = first sorted slot of cell c (boundary fill)
+#include <algorithm>
+#include <cmath>
+
+#include "radix_sort.cuh"
+#include "sjcs_internal.cuh"
+
+namespace sjcs {
+namespace {
+
+struct KeysFromParticles {
+    const float* __restrict__ xyz;
+    GridGeom g;
+    __device__ __forceinline__ uint32_t operator()(uint64_t i) const {
+        return cell_key(g, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    }
+};
+
+// Last pass: write the sorted key and gather the particle into SoA slot g.
+struct SinkGatherParticles {
+    const float* __restrict__ xyz;
+    uint32_t* __restrict__ keys;
+    float* __restrict__ xs;
+    float* __restrict__ ys;
+    float* __restrict__ zs;
+    __device__ __forceinline__ void operator()(uint32_t g, uint32_t k, uint32_t v) const {
+        keys[g] = k;
+        const uint64_t s = 3ull * v;
+        xs[g] = xyz[s];
+        ys[g] = xyz[s + 1];
+        zs[g] = xyz[s + 2];
+    }
+};
+
+struct Gap {
+    uint32_t lo, hi, val;  // cells [lo, hi] start at slot val
+};
+constexpr uint32_t kGapInline = 64;
+
+// cell_start[c] = i for every cell c in (key[i-1], key[i]] (key[-1] = -1,
+// key[n] = ncells), so empty cells point at the next occupied slot and
+// cell_start[ncells] = n.  Long runs of empty cells go to a gap list that a
+// second kernel fills cooperatively.
+__global__ void k_cell_start(const uint32_t* __restrict__ keys, uint64_t n, uint64_t ncells,
+                             uint32_t* __restrict__ cs, Gap* __restrict__ gaps,
+                             uint32_t* __restrict__ ngaps, uint32_t max_gaps) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i > n) return;
+    const uint64_t lo = (i == 0) ? 0ull : (uint64_t)keys[i - 1] + 1ull;
+    const uint64_t hi = (i == n) ? ncells : (uint64_t)keys[i];
+    if (lo > hi) return;
+    const uint64_t cnt = hi - lo + 1;
+    const uint64_t inl = cnt < kGapInline ? cnt : kGapInline;
+    for (uint64_t c = 0; c < inl; ++c) cs[lo + c] = (uint32_t)i;
+    if (cnt > kGapInline) {
+        const uint32_t slot = atomicAdd(ngaps, 1u);
+        if (slot < max_gaps) {
+            gaps[slot] = Gap{(uint32_t)(lo + kGapInline), (uint32_t)hi, (uint32_t)i};
+        } else {
+            for (uint64_t c = lo + kGapInline; c <= hi; ++c) cs[c] = (uint32_t)i;
+        }
+    }
+}
+
+__global__ void k_fill_gaps(const Gap* __restrict__ gaps, const uint32_t* __restrict__ ngaps,
+                            uint32_t max_gaps, uint32_t* __restrict__ cs) {
+    const uint32_t ng = min(*ngaps, max_gaps);
+    for (uint32_t gi = blockIdx.x; gi < ng; gi += gridDim.x) {
+        const Gap gp = gaps[gi];
+        for (uint64_t c = (uint64_t)gp.lo + threadIdx.x; c <= gp.hi; c += blockDim.x) cs[c] = gp.val;
+    }
+}
+
+}  // namespace
+
+GridGeom auto_grid(uint64_t n, float radius_hint, const uint32_t* grid_req) {
+    GridGeom g{};
+    int G[3];
+    if (grid_req && grid_req[0] && grid_req[1] && grid_req[2]) {
+        for (int a = 0; a < 3; ++a) G[a] = (int)grid_req[a];
+    } else {
+        // Rows of cells run along x and are looked up with two offsets, so x
+        // can be finer than y/z for free: cells are 2.5x longer in y and z.
+        // Target about 1.6 cells per particle, at most 2^28 cells, and keep
+        // y/z cells >= R/2 so a query box spans at most ~5x5 rows.
+        const double target = std::min(std::max(1.6 * (double)n, 4096.0), 268435456.0);
+        double hyz = std::cbrt(2.5e9 / target);
+        if (radius_hint > 0.0f) hyz = std::max(hyz, 0.5 * (double)radius_hint);
+        const double hx = hyz / 2.5;
+        G[0] = (int)std::min(std::max(std::ceil(1000.0 / hx), 1.0), 4096.0);
+        G[1] = (int)std::min(std::max(std::ceil(1000.0 / hyz), 1.0), 4096.0);
+        G[2] = G[1];
+        while ((uint64_t)G[0] * G[1] * G[2] > 268435456ull) {
+            G[0] = std::max(1, G[0] * 7 / 8);
+            G[1] = std::max(1, G[1] * 7 / 8);
+            G[2] = G[1];
+        }
+    }
+    for (int a = 0; a < 3; ++a) {
+        g.G[a] = G[a];
+        g.inv_h[a] = (float)G[a] / 1000.0f;
+    }
+    g.ncells = (uint64_t)G[0] * G[1] * G[2];
+    return g;
+}
+
+int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGeom& g,
+                     sjcs_index* idx, cudaStream_t s) {
+    (void)ctx;
+    idx->geom = g;
+    const uint64_t nalloc = n ? n : 1;
+    SJCS_CUDA_TRY(cudaMallocAsync(&idx->xs, nalloc * sizeof(float), s));
+    SJCS_CUDA_TRY(cudaMallocAsync(&idx->ys, nalloc * sizeof(float), s));
+    SJCS_CUDA_TRY(cudaMallocAsync(&idx->zs, nalloc * sizeof(float), s));
+    SJCS_CUDA_TRY(cudaMallocAsync(&idx->cell_start, (g.ncells + 1) * sizeof(uint32_t), s));
+
+    uint32_t *ka = nullptr, *kb = nullptr, *va = nullptr, *vb = nullptr, *hist = nullptr;
+    Gap* gaps = nullptr;
+    uint32_t* ngaps = nullptr;
+    const uint32_t max_gaps = 1u << 16;
+    const uint64_t ntiles64 = (n + RS_TILE - 1) / RS_TILE;
+    const uint32_t ntiles = (uint32_t)ntiles64;
+    StreamScratch scr(s);  // freed (stream-ordered) on every return path
+    SJCS_CUDA_TRY(scr.alloc(&ka, nalloc * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&kb, nalloc * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&va, nalloc * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&vb, nalloc * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&hist, ((uint64_t)RS_BINS * (ntiles ? ntiles : 1)) * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&gaps, max_gaps * sizeof(Gap)));
+    SJCS_CUDA_TRY(scr.alloc(&ngaps, sizeof(uint32_t)));
+    SJCS_CUDA_TRY(cudaMemsetAsync(ngaps, 0, sizeof(uint32_t), s));
+
+    uint32_t* sorted_keys = ka;
+    if (n > 0) {
+        int key_bits = 1;
+        while (key_bits < 32 && (1ull << key_bits) < g.ncells) ++key_bits;
+        const int passes = (key_bits + RS_BITS - 1) / RS_BITS;
+        const KeysFromParticles kp{d_xyz, g};
+        uint32_t *kin = nullptr, *vin = nullptr, *kout = ka, *vout = va;
+        for (int p = 0; p < passes; ++p) {
+            const int shift = p * RS_BITS;
+            const bool first = (p == 0), last = (p == passes - 1);
+            if (first)
+                k_radix_upsweep<<<ntiles, RS_THREADS, 0, s>>>(kp, n, shift, hist, ntiles);
+            else
+                k_radix_upsweep<<<ntiles, RS_THREADS, 0, s>>>(KeysFromArray{kin}, n, shift, hist, ntiles);
+            SJCS_LAUNCH_CHECK();
+            int rc = exclusive_scan_u32(hist, (uint64_t)RS_BINS * ntiles, s);
+            if (rc) return rc;
+            if (last) {
+                const SinkGatherParticles sink{d_xyz, kout, idx->xs, idx->ys, idx->zs};
+                if (first)
+                    k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(kp, ValsIota{}, n, shift, hist, ntiles, sink);
+                else
+                    k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(KeysFromArray{kin}, ValsFromArray{vin}, n,
+                                                                     shift, hist, ntiles, sink);
+            } else {
+                const SinkPairs sink{kout, vout};
+                if (first)
+                    k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(kp, ValsIota{}, n, shift, hist, ntiles, sink);
+                else
+                    k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(KeysFromArray{kin}, ValsFromArray{vin}, n,
+                                                                     shift, hist, ntiles, sink);
+            }
+            SJCS_LAUNCH_CHECK();
+            sorted_keys = kout;
+            kin = kout;
+            vin = vout;
+            kout = (kout == ka) ? kb : ka;
+            vout = (vout == va) ? vb : va;
+        }
+    }
+    {
+        const uint64_t threads = n + 1;
+        const unsigned blocks = (unsigned)((threads + 255) / 256);
+        k_cell_start<<<blocks, 256, 0, s>>>(sorted_keys, n, g.ncells, idx->cell_start, gaps, ngaps, max_gaps);
+        SJCS_LAUNCH_CHECK();
+        k_fill_gaps<<<1024, 256, 0, s>>>(gaps, ngaps, max_gaps, idx->cell_start);
+        SJCS_LAUNCH_CHECK();
+    }
+    return SJCS_OK;
+}
+
+}  // namespace sjcs

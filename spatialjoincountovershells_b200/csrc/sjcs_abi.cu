@@ -1,0 +1,599 @@
+// extern "C" entry points of libsjcs.so (declared in include/sjcs.h).
+#include <algorithm>
+#include <atomic>
+#include <cmath>
+#include <cstdarg>
+#include <cstring>
+#include <new>
+#include <thread>
+
+#include "sjcs_internal.cuh"
+
+namespace sjcs {
+
+static thread_local std::string g_last_error;
+static std::atomic<uint64_t> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+}
+
+int fail(int code, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+namespace {
+
+__global__ void k_widen_u32_u64(const uint32_t* __restrict__ in, uint64_t m, unsigned long long* __restrict__ out) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) out[i] = in[i];
+}
+
+__global__ void k_fill_f32(float* __restrict__ p, uint64_t m, float v) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < m) p[i] = v;
+}
+
+bool valid_ctx(const sjcs_ctx* c) { return c && c->magic == kCtxMagic; }
+bool valid_index(const sjcs_index* i) { return i && i->magic == kIndexMagic; }
+bool valid_query(const sjcs_query* q) { return q && q->magic == kQueryMagic; }
+
+int set_device(const sjcs_ctx* ctx) {
+    SJCS_CUDA_TRY(cudaSetDevice(ctx->device));
+    return SJCS_OK;
+}
+
+bool is_pinned(const void* p) {
+    cudaPointerAttributes a;
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    return a.type == cudaMemoryTypeHost;
+}
+
+// Parallel host copy/add of a widened chunk into the caller's array.
+void host_store(uint64_t* dst, const uint64_t* src, uint64_t m, bool add) {
+    const unsigned hw = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    const unsigned nt = (m < (1u << 20)) ? 1u : hw;
+    auto work = [&](unsigned t) {
+        const uint64_t lo = m * t / nt, hi = m * (t + 1) / nt;
+        if (add)
+            for (uint64_t i = lo; i < hi; ++i) dst[i] += src[i];
+        else
+            std::memcpy(dst + lo, src + lo, (hi - lo) * sizeof(uint64_t));
+    };
+    if (nt == 1) {
+        work(0);
+        return;
+    }
+    std::vector<std::thread> th;
+    th.reserve(nt);
+    for (unsigned t = 0; t < nt; ++t) th.emplace_back(work, t);
+    for (auto& x : th) x.join();
+}
+
+int query_prepare(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride, uint64_t nhalos, const float* r2,
+                  int nrads, int flags, sjcs_query* q, StreamScratch* keep) {
+    (void)keep;
+    cudaStream_t s = ctx->s_count;
+    q->nhalos = nhalos;
+    q->nrads = nrads;
+    q->flags = flags;
+    int pad = 1;
+    while (pad < nrads) pad <<= 1;
+    q->pad = pad;
+    bool mono = true;
+    for (int i = 0; i < nrads; ++i) {
+        if (std::isnan(r2[i])) mono = false;
+        if (i + 1 < nrads && !(r2[i] <= r2[i + 1])) mono = false;
+    }
+    q->monotone = mono;
+    q->r2max = r2[nrads - 1];
+    q->R = (float)std::sqrt((double)r2[nrads - 1]);
+    q->half = (flags & SJCS_QUERY_PERIODIC) ? q->R : r2[nrads - 1];
+    SJCS_CUDA_TRY(cudaMallocAsync(&q->d_r2, (size_t)pad * sizeof(float), s));
+    k_fill_f32<<<(pad + 255) / 256, 256, 0, s>>>(q->d_r2, (uint64_t)pad, INFINITY);
+    SJCS_LAUNCH_CHECK();
+    SJCS_CUDA_TRY(cudaMemcpyAsync(q->d_r2, r2, (size_t)nrads * sizeof(float), cudaMemcpyHostToDevice, s));
+    const uint64_t ncnt = nhalos * (uint64_t)nrads;
+    SJCS_CUDA_TRY(cudaMallocAsync(&q->counts, (ncnt ? ncnt : 1) * sizeof(uint32_t), s));
+    if (ncnt) SJCS_CUDA_TRY(cudaMemsetAsync(q->counts, 0, ncnt * sizeof(uint32_t), s));
+    SJCS_CUDA_TRY(cudaMallocAsync(&q->halos, (nhalos ? nhalos : 1) * sizeof(float4), s));
+    return sort_halos(ctx, d_halo_xyz, stride, nhalos, q->halos, s);
+}
+
+int check_query_args(sjcs_ctx* ctx, const float* halo_xyz, size_t stride, uint64_t nhalos, const float* r2,
+                     int nrads, int flags, sjcs_query** out) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!out) return fail(SJCS_ERR_INVALID, "out is NULL");
+    if (nhalos && !halo_xyz) return fail(SJCS_ERR_INVALID, "halo_xyz is NULL");
+    if (!r2 || nrads <= 0) return fail(SJCS_ERR_INVALID, "radius table is empty");
+    if (stride < 3 * sizeof(float) || (stride % sizeof(float)) != 0)
+        return fail(SJCS_ERR_INVALID, "stride_bytes must be a multiple of 4 and >= 12 (got %zu)", stride);
+    if (nhalos > 0xffffffffull) return fail(SJCS_ERR_INVALID, "too many halos (%llu)", (unsigned long long)nhalos);
+    if (flags & ~SJCS_QUERY_PERIODIC) return fail(SJCS_ERR_INVALID, "unknown query flags 0x%x", flags);
+    return SJCS_OK;
+}
+
+void clear_count_events(sjcs_query* q) {
+    for (cudaEvent_t e : q->count_events) cudaEventDestroy(e);
+    q->count_events.clear();
+}
+
+sjcs_query* new_query(sjcs_ctx* ctx) {
+    sjcs_query* q = new (std::nothrow) sjcs_query();
+    if (!q) return nullptr;
+    q->magic = kQueryMagic;
+    q->ctx = ctx;
+    cudaEventCreate(&q->ev_last);
+    cudaEventCreate(&q->ev_d0);
+    cudaEventCreate(&q->ev_d1);
+    return q;
+}
+
+void free_query(sjcs_query* q) {
+    if (!q) return;
+    cudaStream_t s = q->ctx->s_count;
+    if (q->halos) cudaFreeAsync(q->halos, s);
+    if (q->counts) cudaFreeAsync(q->counts, s);
+    if (q->d_r2) cudaFreeAsync(q->d_r2, s);
+    cudaStreamSynchronize(s);
+    if (q->h_stage) cudaFreeHost(q->h_stage);
+    clear_count_events(q);
+    cudaEventDestroy(q->ev_last);
+    cudaEventDestroy(q->ev_d0);
+    cudaEventDestroy(q->ev_d1);
+    q->magic = 0;
+    delete q;
+}
+
+sjcs_index* new_index(sjcs_ctx* ctx) {
+    sjcs_index* idx = new (std::nothrow) sjcs_index();
+    if (!idx) return nullptr;
+    idx->magic = kIndexMagic;
+    idx->ctx = ctx;
+    cudaEventCreate(&idx->ev_start);
+    cudaEventCreate(&idx->ev_h2d);
+    cudaEventCreate(&idx->ev_ready);
+    return idx;
+}
+
+void free_index(sjcs_index* idx) {
+    if (!idx) return;
+    sjcs_ctx* ctx = idx->ctx;
+    // Frees are ordered after the build (build stream) and after every count
+    // queued on the count stream that reads this index.
+    cudaStreamWaitEvent(ctx->s_count, idx->ev_ready, 0);
+    if (idx->xs) cudaFreeAsync(idx->xs, ctx->s_count);
+    if (idx->ys) cudaFreeAsync(idx->ys, ctx->s_count);
+    if (idx->zs) cudaFreeAsync(idx->zs, ctx->s_count);
+    if (idx->cell_start) cudaFreeAsync(idx->cell_start, ctx->s_count);
+    cudaEventDestroy(idx->ev_start);
+    cudaEventDestroy(idx->ev_h2d);
+    cudaEventDestroy(idx->ev_ready);
+    idx->magic = 0;
+    delete idx;
+}
+
+int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, const sjcs_index_opts* opts,
+                       sjcs_index** out) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!out) return fail(SJCS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (n && !xyz) return fail(SJCS_ERR_INVALID, "xyz is NULL");
+    if (n > 0xffffffffull) return fail(SJCS_ERR_INVALID, "too many particles for one index (%llu)", (unsigned long long)n);
+    sjcs_index_opts o{};
+    if (opts) o = *opts;
+    if (o.kind != SJCS_INDEX_GRID) return fail(SJCS_ERR_INVALID, "unsupported index kind %d", o.kind);
+    for (int i = 0; i < 4; ++i)
+        if (o.reserved[i]) return fail(SJCS_ERR_INVALID, "reserved option fields must be zero");
+    if (!(o.radius_hint >= 0.0f)) return fail(SJCS_ERR_INVALID, "radius_hint must be >= 0");
+    if ((o.grid[0] || o.grid[1] || o.grid[2]) &&
+        (!o.grid[0] || !o.grid[1] || !o.grid[2] || o.grid[0] > 65535 || o.grid[1] > 65535 || o.grid[2] > 65535 ||
+         (uint64_t)o.grid[0] * o.grid[1] * o.grid[2] > (1ull << 31)))
+        return fail(SJCS_ERR_INVALID, "grid must be all zero or three values in [1,65535] with <= 2^31 cells");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    sjcs_index* idx = new_index(ctx);
+    if (!idx) return fail(SJCS_ERR_NOMEM, "out of host memory");
+    idx->kind = o.kind;
+    idx->n = n;
+    cudaStream_t s = ctx->s_build;
+    cudaEventRecord(idx->ev_start, s);
+    const float* d_xyz = xyz;
+    StreamScratch scr(s);
+    if (host && n) {
+        float* d = nullptr;
+        cudaError_t e = scr.alloc(&d, n * 3 * sizeof(float));
+        if (e != cudaSuccess) {
+            free_index(idx);
+            return fail(SJCS_ERR_NOMEM, "device allocation of %llu particles failed: %s", (unsigned long long)n,
+                        cudaGetErrorString(e));
+        }
+        e = cudaMemcpyAsync(d, xyz, n * 3 * sizeof(float), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            free_index(idx);
+            return fail(SJCS_ERR_CUDA, "host-to-device copy failed: %s", cudaGetErrorString(e));
+        }
+        d_xyz = d;
+        idx->had_h2d = true;
+    }
+    cudaEventRecord(idx->ev_h2d, s);
+    const GridGeom g = auto_grid(n, o.radius_hint, o.grid);
+    rc = build_grid_index(ctx, d_xyz, n, g, idx, s);
+    if (rc) {
+        free_index(idx);
+        return rc;
+    }
+    cudaEventRecord(idx->ev_ready, s);
+    *out = idx;
+    return SJCS_OK;
+}
+
+}  // namespace
+}  // namespace sjcs
+
+using namespace sjcs;
+
+extern "C" {
+
+const char* sjcs_last_error(void) { return g_last_error.c_str(); }
+
+const char* sjcs_version(void) { return "sjcs-b200 0.1 (sm_100a)"; }
+
+int sjcs_ctx_create(int device, sjcs_ctx** out) {
+    if (!out) return fail(SJCS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    int ndev = 0;
+    cudaError_t e = cudaGetDeviceCount(&ndev);
+    if (e != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(SJCS_ERR_CUDA, "no CUDA device available (%s)", cudaGetErrorString(e));
+    }
+    if (device < 0 || device >= ndev) return fail(SJCS_ERR_INVALID, "device %d out of range [0,%d)", device, ndev);
+    SJCS_CUDA_TRY(cudaSetDevice(device));
+    int major = 0;
+    SJCS_CUDA_TRY(cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, device));
+    if (major < 10) return fail(SJCS_ERR_CUDA, "device %d is sm_%d0-class; this library is built for sm_100a", device, major);
+    sjcs_ctx* ctx = new (std::nothrow) sjcs_ctx();
+    if (!ctx) return fail(SJCS_ERR_NOMEM, "out of host memory");
+    ctx->magic = kCtxMagic;
+    ctx->device = device;
+    cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
+    SJCS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->s_build, cudaStreamNonBlocking));
+    SJCS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->s_count, cudaStreamNonBlocking));
+    // Keep freed stream-ordered memory cached in the pool: every file's index
+    // and scratch reuse the previous file's pages without new cudaMalloc calls.
+    cudaMemPool_t pool;
+    if (cudaDeviceGetDefaultMemPool(&pool, device) == cudaSuccess) {
+        uint64_t thr = UINT64_MAX;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &thr);
+    }
+    cudaGetLastError();
+    *out = ctx;
+    return SJCS_OK;
+}
+
+int sjcs_ctx_destroy(sjcs_ctx* ctx) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    cudaSetDevice(ctx->device);
+    cudaStreamSynchronize(ctx->s_build);
+    cudaStreamSynchronize(ctx->s_count);
+    cudaStreamDestroy(ctx->s_build);
+    cudaStreamDestroy(ctx->s_count);
+    ctx->magic = 0;
+    delete ctx;
+    return SJCS_OK;
+}
+
+int sjcs_ctx_sync(sjcs_ctx* ctx) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_build));
+    SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_count));
+    return SJCS_OK;
+}
+
+int sjcs_ctx_stream(const sjcs_ctx* ctx, int which, void** stream) {
+    if (!valid_ctx(ctx) || !stream || (which != 0 && which != 1)) return fail(SJCS_ERR_INVALID, "invalid argument");
+    *stream = (void*)(which == 0 ? ctx->s_build : ctx->s_count);
+    return SJCS_OK;
+}
+
+uint64_t sjcs_launch_counter(void) { return g_launches.load(); }
+
+int sjcs_ctx_num_sms(const sjcs_ctx* ctx, int* out) {
+    if (!valid_ctx(ctx) || !out) return fail(SJCS_ERR_INVALID, "invalid argument");
+    *out = ctx->num_sms;
+    return SJCS_OK;
+}
+
+int sjcs_host_alloc(size_t bytes, void** out) {
+    if (!out) return fail(SJCS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    cudaError_t e = cudaMallocHost(out, bytes ? bytes : 1);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SJCS_ERR_NOMEM, "pinned allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+    }
+    return SJCS_OK;
+}
+
+int sjcs_host_free(void* p) {
+    if (!p) return SJCS_OK;
+    SJCS_CUDA_TRY(cudaFreeHost(p));
+    return SJCS_OK;
+}
+
+int sjcs_index_build(sjcs_ctx* ctx, const float* xyz, uint64_t n, const sjcs_index_opts* opts, sjcs_index** out) {
+    return index_build_common(ctx, xyz, true, n, opts, out);
+}
+
+int sjcs_index_build_device(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const sjcs_index_opts* opts,
+                            sjcs_index** out) {
+    return index_build_common(ctx, d_xyz, false, n, opts, out);
+}
+
+int sjcs_index_wait(sjcs_index* idx) {
+    if (!valid_index(idx)) return fail(SJCS_ERR_STATE, "invalid index");
+    SJCS_CUDA_TRY(cudaEventSynchronize(idx->ev_ready));
+    return SJCS_OK;
+}
+
+int sjcs_index_size(const sjcs_index* idx, uint64_t* out) {
+    if (!valid_index(idx) || !out) return fail(SJCS_ERR_INVALID, "invalid argument");
+    *out = idx->n;
+    return SJCS_OK;
+}
+
+int sjcs_index_grid(const sjcs_index* idx, uint32_t out[3]) {
+    if (!valid_index(idx) || !out) return fail(SJCS_ERR_INVALID, "invalid argument");
+    for (int a = 0; a < 3; ++a) out[a] = (uint32_t)idx->geom.G[a];
+    return SJCS_OK;
+}
+
+int sjcs_index_timing(const sjcs_index* idx, sjcs_timing* out) {
+    if (!valid_index(idx) || !out) return fail(SJCS_ERR_INVALID, "invalid argument");
+    SJCS_CUDA_TRY(cudaEventSynchronize(idx->ev_ready));
+    sjcs_timing t{};
+    float ms = 0.f;
+    if (idx->had_h2d && cudaEventElapsedTime(&ms, idx->ev_start, idx->ev_h2d) == cudaSuccess) t.h2d_ms = ms;
+    if (cudaEventElapsedTime(&ms, idx->ev_h2d, idx->ev_ready) == cudaSuccess) t.build_ms = ms;
+    cudaGetLastError();
+    *out = t;
+    return SJCS_OK;
+}
+
+int sjcs_index_destroy(sjcs_index* idx) {
+    if (!valid_index(idx)) return fail(SJCS_ERR_STATE, "invalid index");
+    sjcs_ctx* ctx = idx->ctx;
+    cudaSetDevice(ctx->device);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    free_index(idx);
+    return SJCS_OK;
+}
+
+int sjcs_query_create(sjcs_ctx* ctx, const float* halo_xyz, size_t stride_bytes, uint64_t nhalos, const float* r2,
+                      int nrads, int flags, sjcs_query** out) {
+    int rc = check_query_args(ctx, halo_xyz, stride_bytes, nhalos, r2, nrads, flags, out);
+    if (rc) return rc;
+    *out = nullptr;
+    rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    sjcs_query* q = new_query(ctx);
+    if (!q) return fail(SJCS_ERR_NOMEM, "out of host memory");
+    cudaStream_t s = ctx->s_count;
+    StreamScratch scr(s);
+    float* d_raw = nullptr;
+    // The last halo needs only its 12 coordinate bytes, not a whole stride.
+    const size_t bytes = nhalos ? (size_t)(nhalos - 1) * stride_bytes + 3 * sizeof(float) : 0;
+    if (nhalos) {
+        cudaError_t e = scr.alloc(&d_raw, bytes);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_raw, halo_xyz, bytes, cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            free_query(q);
+            return fail(SJCS_ERR_CUDA, "halo upload failed: %s", cudaGetErrorString(e));
+        }
+    }
+    rc = query_prepare(ctx, d_raw, stride_bytes, nhalos, r2, nrads, flags, q, &scr);
+    if (rc) {
+        free_query(q);
+        return rc;
+    }
+    *out = q;
+    return SJCS_OK;
+}
+
+int sjcs_query_create_device(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride_bytes, uint64_t nhalos,
+                             const float* r2, int nrads, int flags, sjcs_query** out) {
+    int rc = check_query_args(ctx, d_halo_xyz, stride_bytes, nhalos, r2, nrads, flags, out);
+    if (rc) return rc;
+    *out = nullptr;
+    rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    sjcs_query* q = new_query(ctx);
+    if (!q) return fail(SJCS_ERR_NOMEM, "out of host memory");
+    rc = query_prepare(ctx, d_halo_xyz, stride_bytes, nhalos, r2, nrads, flags, q, nullptr);
+    if (rc) {
+        free_query(q);
+        return rc;
+    }
+    *out = q;
+    return SJCS_OK;
+}
+
+int sjcs_query_count(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_query(q) || q->ctx != ctx) return fail(SJCS_ERR_STATE, "query does not belong to this context");
+    if (!valid_index(idx) || idx->ctx != ctx) return fail(SJCS_ERR_STATE, "index does not belong to this context");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t s = ctx->s_count;
+    SJCS_CUDA_TRY(cudaStreamWaitEvent(s, idx->ev_ready, 0));
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    SJCS_CUDA_TRY(cudaEventCreate(&e0));
+    SJCS_CUDA_TRY(cudaEventCreate(&e1));
+    q->count_events.push_back(e0);
+    q->count_events.push_back(e1);
+    cudaEventRecord(e0, s);
+    rc = launch_shell_count(ctx, q, idx, s);
+    cudaEventRecord(e1, s);
+    cudaEventRecord(q->ev_last, s);
+    return rc;
+}
+
+int sjcs_query_wait(sjcs_query* q) {
+    if (!valid_query(q)) return fail(SJCS_ERR_STATE, "invalid query");
+    SJCS_CUDA_TRY(cudaEventSynchronize(q->ev_last));
+    return SJCS_OK;
+}
+
+int sjcs_query_read_counts(sjcs_ctx* ctx, sjcs_query* q, uint64_t* counts, int accumulate) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_query(q) || q->ctx != ctx) return fail(SJCS_ERR_STATE, "query does not belong to this context");
+    const uint64_t m = q->nhalos * (uint64_t)q->nrads;
+    if (m && !counts) return fail(SJCS_ERR_INVALID, "counts is NULL");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t s = ctx->s_count;
+    if (m == 0) return SJCS_OK;
+    StreamScratch scr(s);
+    unsigned long long* wide = nullptr;
+    SJCS_CUDA_TRY(scr.alloc(&wide, m * sizeof(uint64_t)));
+    cudaEventRecord(q->ev_d0, s);
+    k_widen_u32_u64<<<ctx->num_sms * 8, 256, 0, s>>>(q->counts, m, wide);
+    SJCS_LAUNCH_CHECK();
+    if (!accumulate && is_pinned(counts)) {
+        SJCS_CUDA_TRY(cudaMemcpyAsync(counts, wide, m * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+        cudaEventRecord(q->ev_d1, s);
+        SJCS_CUDA_TRY(cudaStreamSynchronize(s));
+    } else {
+        // Double-buffered pinned staging; host threads store (or add) chunk
+        // k while the copy engine brings chunk k+1.
+        const uint64_t chunk = 8ull << 20;  // elements (64 MB)
+        if (!q->h_stage) {
+            SJCS_CUDA_TRY(cudaMallocHost(&q->h_stage, 2 * chunk * sizeof(uint64_t)));
+            q->h_stage_elems = 2 * chunk;
+        }
+        uint64_t* stage = reinterpret_cast<uint64_t*>(q->h_stage);
+        cudaEvent_t done[2];
+        cudaEventCreateWithFlags(&done[0], cudaEventDisableTiming);
+        cudaEventCreateWithFlags(&done[1], cudaEventDisableTiming);
+        const uint64_t nchunks = (m + chunk - 1) / chunk;
+        int err = SJCS_OK;
+        for (uint64_t c = 0; c <= nchunks && !err; ++c) {
+            if (c < nchunks) {
+                const uint64_t off = c * chunk, len = std::min(chunk, m - off);
+                cudaError_t e = cudaMemcpyAsync(stage + (c & 1) * chunk, wide + off, len * sizeof(uint64_t),
+                                                cudaMemcpyDeviceToHost, s);
+                if (e == cudaSuccess) e = cudaEventRecord(done[c & 1], s);
+                if (e != cudaSuccess) err = fail(SJCS_ERR_CUDA, "count read-back failed: %s", cudaGetErrorString(e));
+            }
+            if (c > 0 && !err) {
+                const uint64_t p = c - 1, off = p * chunk, len = std::min(chunk, m - off);
+                cudaError_t e = cudaEventSynchronize(done[p & 1]);
+                if (e != cudaSuccess) err = fail(SJCS_ERR_CUDA, "count read-back failed: %s", cudaGetErrorString(e));
+                else host_store(counts + off, stage + (p & 1) * chunk, len, accumulate != 0);
+            }
+        }
+        cudaEventRecord(q->ev_d1, s);
+        cudaStreamSynchronize(s);
+        cudaEventDestroy(done[0]);
+        cudaEventDestroy(done[1]);
+        if (err) return err;
+    }
+    float ms = 0.f;
+    q->last_d2h_ms = (cudaEventElapsedTime(&ms, q->ev_d0, q->ev_d1) == cudaSuccess) ? ms : 0.f;
+    cudaGetLastError();
+    return SJCS_OK;
+}
+
+int sjcs_query_device_counts(const sjcs_query* q, uint32_t** d_counts) {
+    if (!valid_query(q) || !d_counts) return fail(SJCS_ERR_INVALID, "invalid argument");
+    *d_counts = q->counts;
+    return SJCS_OK;
+}
+
+int sjcs_query_reset(sjcs_ctx* ctx, sjcs_query* q) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_query(q) || q->ctx != ctx) return fail(SJCS_ERR_STATE, "query does not belong to this context");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    const uint64_t m = q->nhalos * (uint64_t)q->nrads;
+    if (m) SJCS_CUDA_TRY(cudaMemsetAsync(q->counts, 0, m * sizeof(uint32_t), ctx->s_count));
+    SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_count));
+    clear_count_events(q);
+    return SJCS_OK;
+}
+
+int sjcs_query_timing(const sjcs_query* q, sjcs_timing* out) {
+    if (!valid_query(q) || !out) return fail(SJCS_ERR_INVALID, "invalid argument");
+    SJCS_CUDA_TRY(cudaEventSynchronize(q->ev_last));
+    sjcs_timing t{};
+    for (size_t i = 0; i + 1 < q->count_events.size(); i += 2) {
+        float ms = 0.f;
+        if (cudaEventElapsedTime(&ms, q->count_events[i], q->count_events[i + 1]) == cudaSuccess) t.count_ms += ms;
+        t.count_calls++;
+    }
+    t.d2h_ms = q->last_d2h_ms;
+    cudaGetLastError();
+    *out = t;
+    return SJCS_OK;
+}
+
+int sjcs_query_destroy(sjcs_query* q) {
+    if (!valid_query(q)) return fail(SJCS_ERR_STATE, "invalid query");
+    sjcs_ctx* ctx = q->ctx;
+    cudaSetDevice(ctx->device);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    free_query(q);
+    return SJCS_OK;
+}
+
+int sjcs_multi_range_count(sjcs_ctx* ctx, const sjcs_index* idx, const float* halo_xyz, size_t stride_bytes,
+                           uint64_t nhalos, const float* r2, int nrads, int flags, uint64_t* counts) {
+    if (nhalos && !counts) return fail(SJCS_ERR_INVALID, "counts is NULL");
+    sjcs_query* q = nullptr;
+    int rc = sjcs_query_create(ctx, halo_xyz, stride_bytes, nhalos, r2, nrads, flags, &q);
+    if (rc) return rc;
+    rc = sjcs_query_count(ctx, q, idx);
+    if (!rc) rc = sjcs_query_read_counts(ctx, q, counts, 1);
+    sjcs_query_destroy(q);
+    return rc;
+}
+
+int sjcs_radius_table(double minrad, double maxrad, int nrads, float* r2) {
+    if (nrads <= 0 || !r2) return fail(SJCS_ERR_INVALID, "nrads must be > 0 and r2 non-NULL");
+    if (minrad > maxrad) std::swap(minrad, maxrad);
+    // Logspace(2.0, log2(min), log2(max), n, r): the reference is built with
+    // -O2 -march=native, which contracts a + i*c into one fused multiply-add.
+    const double a = std::log2(minrad), b = std::log2(maxrad);
+    const double c = (b - a) / (nrads - 1);
+    for (int i = 0; i < nrads - 1; ++i) r2[i] = (float)std::pow(2.0, std::fma((double)i, c, a));
+    r2[nrads - 1] = (float)std::pow(2.0, b);
+    for (int i = 0; i < nrads; ++i) r2[i] = r2[i] * r2[i];
+    return SJCS_OK;
+}
+
+}  // extern "C"

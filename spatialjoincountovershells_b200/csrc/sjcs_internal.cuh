@@ -1,0 +1,179 @@
+// Internal declarations shared by the CUDA translation units of libsjcs.so.
+//
+// Data layout in HBM (one particle file = one index):
+//   xs[n], ys[n], zs[n]   fp32, particles sorted by cell key (SoA, so a warp
+//                         reading 32 consecutive candidates touches 3 x 128 B)
+//   cell_start[ncells+1]  u32, first sorted slot of every cell; cells are
+//                         numbered x-fastest ((cz*Gy + cy)*Gx + cx), so one
+//                         (cy, cz) row of cells is one contiguous slot range.
+// A query holds the halos sorted along a Morton curve (float4 x,y,z,orig-id)
+// and u32 count accumulators [nhalos][nrads] in the caller's halo order.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/sjcs.h"
+
+namespace sjcs {
+
+// Periodic box edge of the reference (LOW_BOUND / UPP_BOUND,
+// include/objects/RTree/Mbr.h:7-8).
+constexpr float kBoxLow = 0.0f;
+constexpr float kBoxUpp = 1000.0f;
+
+void set_error(const char* fmt, ...);
+int fail(int code, const char* fmt, ...);
+void note_launch();  // counts this library's kernel launches (sjcs_launch_counter)
+
+#define SJCS_CUDA_TRY(expr)                                                            \
+    do {                                                                               \
+        cudaError_t e_ = (expr);                                                       \
+        if (e_ != cudaSuccess)                                                         \
+            return ::sjcs::fail(SJCS_ERR_CUDA, "%s:%d: %s: %s", __FILE__, __LINE__,   \
+                                #expr, cudaGetErrorString(e_));                        \
+    } while (0)
+
+#define SJCS_LAUNCH_CHECK()                                                            \
+    do {                                                                               \
+        ::sjcs::note_launch();                                                         \
+        cudaError_t e_ = cudaGetLastError();                                           \
+        if (e_ != cudaSuccess)                                                         \
+            return ::sjcs::fail(SJCS_ERR_CUDA, "%s:%d: kernel launch: %s", __FILE__,   \
+                                __LINE__, cudaGetErrorString(e_));                     \
+    } while (0)
+
+// Stream-ordered scratch: every buffer allocated through it is released with
+// cudaFreeAsync on the same stream when the holder goes out of scope, so
+// error returns do not leak and no host synchronisation is needed.
+struct StreamScratch {
+    cudaStream_t s;
+    std::vector<void*> ptrs;
+    explicit StreamScratch(cudaStream_t st) : s(st) {}
+    StreamScratch(const StreamScratch&) = delete;
+    StreamScratch& operator=(const StreamScratch&) = delete;
+    template <class T>
+    cudaError_t alloc(T** p, size_t bytes) {
+        cudaError_t e = cudaMallocAsync(reinterpret_cast<void**>(p), bytes ? bytes : 16, s);
+        if (e == cudaSuccess) ptrs.push_back(static_cast<void*>(*p));
+        return e;
+    }
+    ~StreamScratch() {
+        for (void* p : ptrs) cudaFreeAsync(p, s);
+    }
+};
+
+// Uniform cell grid over [0,1000)^3.  Coordinates outside the box clamp into
+// the edge cells, so the cell of any value is monotone in the value and a
+// query box [lo, hi] always covers the cells of every point inside it.
+struct GridGeom {
+    float inv_h[3];   // cells per unit length, G/1000 in fp32
+    int G[3];         // cells per axis
+    uint64_t ncells;  // G[0]*G[1]*G[2]
+};
+
+__device__ __forceinline__ int cell_of(float v, float inv_h, int G) {
+    // __fmul_rn: never contracted, so build and query compute the same cell.
+    float t = floorf(__fmul_rn(v, inv_h));
+    t = fminf(fmaxf(t, 0.0f), (float)(G - 1));  // fmaxf(NaN, 0) == 0
+    return (int)t;
+}
+
+__device__ __forceinline__ uint32_t cell_key(const GridGeom& g, float x, float y, float z) {
+    const uint32_t cx = (uint32_t)cell_of(x, g.inv_h[0], g.G[0]);
+    const uint32_t cy = (uint32_t)cell_of(y, g.inv_h[1], g.G[1]);
+    const uint32_t cz = (uint32_t)cell_of(z, g.inv_h[2], g.G[2]);
+    return (cz * (uint32_t)g.G[1] + cy) * (uint32_t)g.G[0] + cx;
+}
+
+// 10-bit-per-axis Morton code used only to order halos for cache locality.
+__device__ __forceinline__ uint32_t spread3_10(uint32_t v) {
+    v &= 0x3ffu;
+    v = (v | (v << 16)) & 0x030000ffu;
+    v = (v | (v << 8)) & 0x0300f00fu;
+    v = (v | (v << 4)) & 0x030c30c3u;
+    v = (v | (v << 2)) & 0x09249249u;
+    return v;
+}
+__device__ __forceinline__ uint32_t morton30(float x, float y, float z) {
+    const float s = 1024.0f / 1000.0f;
+    const uint32_t qx = (uint32_t)cell_of(x, s, 1024);
+    const uint32_t qy = (uint32_t)cell_of(y, s, 1024);
+    const uint32_t qz = (uint32_t)cell_of(z, s, 1024);
+    return spread3_10(qx) | (spread3_10(qy) << 1) | (spread3_10(qz) << 2);
+}
+
+}  // namespace sjcs
+
+// ---- opaque ABI objects ----------------------------------------------------
+
+struct sjcs_ctx {
+    uint32_t magic;
+    int device;
+    int num_sms;
+    cudaStream_t s_build;  // particle copies + index builds
+    cudaStream_t s_count;  // halo upload/sort, shell counts, count read-back
+    std::mutex mu;
+};
+
+struct sjcs_index {
+    uint32_t magic;
+    sjcs_ctx* ctx;
+    int kind;
+    uint64_t n;
+    sjcs::GridGeom geom;
+    float* xs;
+    float* ys;
+    float* zs;
+    uint32_t* cell_start;  // geom.ncells + 1 entries
+    cudaEvent_t ev_start, ev_h2d, ev_ready;
+    bool had_h2d;
+};
+
+struct sjcs_query {
+    uint32_t magic;
+    sjcs_ctx* ctx;
+    uint64_t nhalos;
+    int nrads;
+    int flags;
+    int pad;            // power of two >= nrads (binary-search table size)
+    bool monotone;      // r2 non-decreasing and free of NaN: fast binning
+    float R;            // (float)sqrt((double)r2[nrads-1]), as MultiRangeCount.c:19
+    float half;         // query half-width: R (periodic) or r2[nrads-1] (non-periodic, MultiRangeCount.c:81)
+    float r2max;
+    float4* halos;      // Morton-sorted halos, .w = original index bits
+    uint32_t* counts;   // [nhalos][nrads], caller's halo order
+    float* d_r2;        // [pad], entries past nrads = +inf
+    uint32_t* h_stage;  // pinned staging for count read-back
+    size_t h_stage_elems;
+    std::vector<cudaEvent_t> count_events;  // (start, end) pairs, one per count call since reset
+    cudaEvent_t ev_last;                    // end of the last count call
+    cudaEvent_t ev_d0, ev_d1;
+    float last_d2h_ms;
+};
+
+namespace sjcs {
+constexpr uint32_t kCtxMagic = 0x534a4358u;    // "SJCX"
+constexpr uint32_t kIndexMagic = 0x534a4958u;  // "SJIX"
+constexpr uint32_t kQueryMagic = 0x534a5158u;  // "SJQX"
+
+// index_build.cu
+int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGeom& g,
+                     sjcs_index* idx, cudaStream_t s);
+GridGeom auto_grid(uint64_t n, float radius_hint, const uint32_t* grid_req);
+
+// query_prep.cu
+int sort_halos(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride_bytes, uint64_t nhalos,
+               float4* out, cudaStream_t s);
+
+// shell_count.cu
+int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx,
+                       cudaStream_t s);
+
+// scan.cu: exclusive prefix sum of m u32 values, in place.
+int exclusive_scan_u32(uint32_t* d_data, uint64_t m, cudaStream_t s);
+}  // namespace sjcs

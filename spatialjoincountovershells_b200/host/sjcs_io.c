@@ -1,0 +1,647 @@
+/*
+ * sjcs_io.c -- reference file formats on the host: decoded particle files,
+ * halo text files (plain and id-filtered), the radius schedule and the result
+ * text.  See include/sjcs_host.h for the format summary.
+ */
+#define _GNU_SOURCE
+#include "../../include/sjcs_host.h"
+
+#include <errno.h>
+#include <fcntl.h>
+#include <math.h>
+#include <pthread.h>
+#include <stdarg.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/mman.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
+/* fgets buffer of the reference's halo reader (BUFSIZE, include/Gadget/BufHalo.h:12) */
+#define LINE_BUF (1024 * 16)
+/* N_HEADER_LINES, include/Gadget/BufHalo.h:8 */
+#define N_HEADER 16
+
+static __thread char g_err[1024];
+
+static int host_fail(const char *fmt, ...)
+{
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(g_err, sizeof(g_err), fmt, ap);
+    va_end(ap);
+    return -1;
+}
+
+const char *sjcs_host_last_error(void) { return g_err; }
+
+static int default_threads(int nthreads)
+{
+    long n;
+    if (nthreads > 0)
+        return nthreads;
+    n = sysconf(_SC_NPROCESSORS_ONLN);
+    if (n < 1)
+        n = 1;
+    if (n > 32)
+        n = 32;
+    return (int)n;
+}
+
+/* ---- particles ------------------------------------------------------------ */
+
+int sjcs_particle_file_count(const char *path, uint64_t *n)
+{
+    struct stat st;
+    if (!path || !n)
+        return host_fail("invalid argument");
+    if (stat(path, &st) != 0)
+        return host_fail("ERROR: file %s not found in readDecodedParticles()", path);
+    *n = (uint64_t)st.st_size / (3 * sizeof(float));
+    return 0;
+}
+
+int sjcs_read_particles(const char *path, float *buf, uint64_t cap, uint64_t *n)
+{
+    uint64_t num, done = 0;
+    int fd;
+    if (sjcs_particle_file_count(path, &num) != 0)
+        return -1;
+    if (num > cap)
+        return host_fail("buffer holds %llu particles, file %s has %llu", (unsigned long long)cap, path,
+                         (unsigned long long)num);
+    fd = open(path, O_RDONLY);
+    if (fd < 0)
+        return host_fail("ERROR: file %s not found in readDecodedParticles()", path);
+    {
+        const uint64_t total = num * 3 * sizeof(float);
+        char *dst = (char *)buf;
+        while (done < total) {
+            ssize_t r = read(fd, dst + done, (size_t)((total - done) > (1u << 30) ? (1u << 30) : (total - done)));
+            if (r <= 0) {
+                close(fd);
+                return host_fail("short read on %s", path);
+            }
+            done += (uint64_t)r;
+        }
+    }
+    close(fd);
+    *n = num;
+    return 0;
+}
+
+int sjcs_write_particle_file(const char *path, const float *xyz, uint64_t n)
+{
+    FILE *fp = fopen(path, "wb");
+    if (!fp)
+        return host_fail("ERROR: cannot open %s", path);
+    if (n && fwrite(xyz, 3 * sizeof(float), n, fp) != n) {
+        fclose(fp);
+        return host_fail("ERROR: while writing %s", path);
+    }
+    if (fclose(fp) != 0)
+        return host_fail("ERROR: while writing %s", path);
+    return 0;
+}
+
+/* ---- halos ---------------------------------------------------------------- */
+
+/* GetDataFromLineFast, src/Gadget/BufHalo.c:218-249: id = strtoul of the
+ * line, mass after the 2nd space, x after 6 more spaces, y and z after one
+ * more each.  str is NUL-terminated like the reference's fgets buffer. */
+static int parse_record(char *str, sjcs_halo *h)
+{
+    int i;
+    h->id = strtoul(str, NULL, 10);
+    for (i = 0; i < 2; i++) {
+        if ((str = strchr(str, ' ')) == NULL)
+            return -1;
+        str++;
+    }
+    h->mass = strtof(str, NULL);
+    for (i = 0; i < 6; i++) {
+        if ((str = strchr(str, ' ')) == NULL)
+            return -1;
+        str++;
+    }
+    h->point[0] = strtof(str, NULL);
+    if ((str = strchr(str, ' ')) == NULL)
+        return -1;
+    str++;
+    h->point[1] = strtof(str, NULL);
+    if ((str = strchr(str, ' ')) == NULL)
+        return -1;
+    str++;
+    h->point[2] = strtof(str, NULL);
+    return 0;
+}
+
+typedef struct HaloVec {
+    sjcs_halo *h;
+    uint64_t n, cap;
+} HaloVec;
+
+static int hv_push(HaloVec *v, const sjcs_halo *h)
+{
+    if (v->n == v->cap) {
+        uint64_t nc = v->cap ? v->cap * 2 : 1024;
+        sjcs_halo *p = realloc(v->h, nc * sizeof(sjcs_halo));
+        if (!p)
+            return -1;
+        v->h = p;
+        v->cap = nc;
+    }
+    v->h[v->n++] = *h;
+    return 0;
+}
+
+/* The reference's reader, literally (readHalos, src/Gadget/BufHalo.c:76-119):
+ * fgets pieces of at most LINE_BUF-1 bytes, 16 header pieces, stop at the
+ * first fgets that reaches end of file. */
+static int read_halos_fgets(const char *path, sjcs_halo **out, uint64_t *n)
+{
+    char tmp[LINE_BUF];
+    FILE *fp;
+    HaloVec v = {0};
+    int row;
+    if ((fp = fopen(path, "r")) == NULL)
+        return host_fail("ERROR: file %s not found in readHalos().", path);
+    tmp[0] = '\0';
+    for (row = 0; row < N_HEADER; row++) {
+        (void)!fgets(tmp, sizeof(tmp), fp);
+        if (feof(fp)) {
+            fclose(fp);
+            return host_fail("ERROR: file %s does not contain headers in readHalos().", path);
+        }
+    }
+    for (;;) {
+        sjcs_halo h;
+        (void)!fgets(tmp, sizeof(tmp), fp);
+        if (feof(fp))
+            break;
+        if (parse_record(tmp, &h) < 0) {
+            fclose(fp);
+            free(v.h);
+            return host_fail("ERROR: contents in file %s may be incorrect in readHalos().", path);
+        }
+        if (hv_push(&v, &h) != 0) {
+            fclose(fp);
+            free(v.h);
+            return host_fail("ERROR: memory shortage in readHalos()");
+        }
+    }
+    fclose(fp);
+    *out = v.h ? v.h : malloc(sizeof(sjcs_halo));
+    *n = v.n;
+    return 0;
+}
+
+typedef struct ParseJob {
+    const char *lo, *hi; /* [lo, hi): whole '\n'-terminated lines */
+    sjcs_halo *dst;      /* NULL in the counting pass */
+    uint64_t nlines;
+    int bad;
+} ParseJob;
+
+static void *parse_job(void *arg)
+{
+    ParseJob *j = arg;
+    const char *p = j->lo;
+    char tmp[LINE_BUF];
+    uint64_t k = 0;
+    while (p < j->hi) {
+        const char *nl = memchr(p, '\n', (size_t)(j->hi - p));
+        size_t len = (size_t)(nl - p) + 1;
+        if (j->dst) {
+            memcpy(tmp, p, len);
+            tmp[len] = '\0';
+            if (parse_record(tmp, &j->dst[k]) < 0) {
+                j->bad = 1;
+                return NULL;
+            }
+        }
+        k++;
+        p = nl + 1;
+    }
+    j->nlines = k;
+    return NULL;
+}
+
+int sjcs_read_halos(const char *path, sjcs_halo **out, uint64_t *n, int nthreads)
+{
+    int fd, T, t, row;
+    struct stat st;
+    const char *base, *p, *end, *data_end;
+    ParseJob *jobs;
+    pthread_t *th;
+    uint64_t total = 0;
+    if (!path || !out || !n)
+        return host_fail("invalid argument");
+    fd = open(path, O_RDONLY);
+    if (fd < 0)
+        return host_fail("ERROR: file %s not found in readHalos().", path);
+    if (fstat(fd, &st) != 0 || st.st_size == 0) {
+        close(fd);
+        return host_fail("ERROR: file %s does not contain headers in readHalos().", path);
+    }
+    base = mmap(NULL, (size_t)st.st_size, PROT_READ, MAP_PRIVATE, fd, 0);
+    close(fd);
+    if (base == MAP_FAILED)
+        return read_halos_fgets(path, out, n);
+    end = base + st.st_size;
+    /* Any line of LINE_BUF-1 bytes or more makes fgets split it into several
+     * records: leave such files to the literal reader. */
+    {
+        const char *q = base;
+        while (q < end) {
+            const char *nl = memchr(q, '\n', (size_t)(end - q));
+            const char *le = nl ? nl + 1 : end;
+            if (le - q >= LINE_BUF - 1) {
+                munmap((void *)base, (size_t)st.st_size);
+                return read_halos_fgets(path, out, n);
+            }
+            q = le;
+        }
+    }
+    /* 16 header lines, each newline-terminated (an unterminated 16th line
+     * makes fgets reach end of file: the reference reports missing headers). */
+    p = base;
+    for (row = 0; row < N_HEADER; row++) {
+        const char *nl = memchr(p, '\n', (size_t)(end - p));
+        if (!nl) {
+            munmap((void *)base, (size_t)st.st_size);
+            return host_fail("ERROR: file %s does not contain headers in readHalos().", path);
+        }
+        p = nl + 1;
+    }
+    /* records: every newline-terminated line; a final unterminated line is
+     * dropped because its fgets reaches end of file. */
+    data_end = end;
+    while (data_end > p && data_end[-1] != '\n')
+        data_end--;
+    T = default_threads(nthreads);
+    if ((uint64_t)(data_end - p) < (1u << 20))
+        T = 1;
+    jobs = calloc(T, sizeof(ParseJob));
+    th = calloc(T, sizeof(pthread_t));
+    if (!jobs || !th) {
+        munmap((void *)base, (size_t)st.st_size);
+        free(jobs);
+        free(th);
+        return host_fail("ERROR: memory shortage in readHalos()");
+    }
+    {
+        const char *q = p;
+        for (t = 0; t < T; t++) {
+            const char *cut = p + (uint64_t)(data_end - p) * (t + 1) / T;
+            if (t == T - 1)
+                cut = data_end;
+            else {
+                if (cut < q)
+                    cut = q;
+                while (cut < data_end && cut[-1] != '\n')
+                    cut++;
+            }
+            jobs[t].lo = q;
+            jobs[t].hi = cut;
+            q = cut;
+        }
+    }
+    for (t = 1; t < T; t++)
+        pthread_create(&th[t], NULL, parse_job, &jobs[t]);
+    parse_job(&jobs[0]);
+    for (t = 1; t < T; t++)
+        pthread_join(th[t], NULL);
+    for (t = 0; t < T; t++)
+        total += jobs[t].nlines;
+    *out = malloc((total ? total : 1) * sizeof(sjcs_halo));
+    if (!*out) {
+        munmap((void *)base, (size_t)st.st_size);
+        free(jobs);
+        free(th);
+        return host_fail("ERROR: memory shortage in readHalos()");
+    }
+    {
+        uint64_t off = 0;
+        for (t = 0; t < T; t++) {
+            jobs[t].dst = *out + off;
+            off += jobs[t].nlines;
+        }
+    }
+    for (t = 1; t < T; t++)
+        pthread_create(&th[t], NULL, parse_job, &jobs[t]);
+    parse_job(&jobs[0]);
+    for (t = 1; t < T; t++)
+        pthread_join(th[t], NULL);
+    munmap((void *)base, (size_t)st.st_size);
+    for (t = 0; t < T; t++) {
+        if (jobs[t].bad) {
+            free(*out);
+            *out = NULL;
+            free(jobs);
+            free(th);
+            return host_fail("ERROR: contents in file %s may be incorrect in readHalos().", path);
+        }
+    }
+    free(jobs);
+    free(th);
+    *n = total;
+    return 0;
+}
+
+void sjcs_host_free_halos(sjcs_halo *h) { free(h); }
+
+static int cmp_u64(const void *a, const void *b)
+{
+    uint64_t x = *(const uint64_t *)a, y = *(const uint64_t *)b;
+    return (x > y) - (x < y);
+}
+
+/* readAndFilterHalos + ConstructFilterIdList, src/Gadget/BufHalo.c:121-214, 132-180 */
+int sjcs_read_and_filter_halos(const char *path, const char *filter_path, sjcs_halo **out, uint64_t *n)
+{
+    char tmp[LINE_BUF];
+    FILE *fp;
+    uint64_t nfilters = 0, row, fr;
+    uint64_t *filter;
+    HaloVec v = {0};
+    int hrow, finished = 0;
+
+    if ((fp = fopen(filter_path, "r")) == NULL)
+        return host_fail("ERROR: file %s not found in ConstructFilterIdList().", filter_path);
+    for (;;) {
+        if (fgets(tmp, sizeof(tmp), fp) == NULL && feof(fp))
+            break;
+        if (ferror(fp)) {
+            fclose(fp);
+            return host_fail("ERROR: while reading %s in ConstructFilterIdList()", filter_path);
+        }
+        nfilters++;
+    }
+    filter = malloc((nfilters ? nfilters : 1) * sizeof(uint64_t));
+    if (!filter) {
+        fclose(fp);
+        return host_fail("ERROR: memory shortage");
+    }
+    rewind(fp);
+    for (row = 0; row < nfilters; row++) {
+        if (fgets(tmp, sizeof(tmp), fp) == NULL && feof(fp))
+            break;
+        filter[row] = (uint64_t)strtol(tmp, NULL, 10);
+    }
+    fclose(fp);
+    /* the reference radix-sorts the ids as unsigned 64-bit keys */
+    qsort(filter, nfilters, sizeof(uint64_t), cmp_u64);
+
+    if ((fp = fopen(path, "r")) == NULL) {
+        free(filter);
+        return host_fail("ERROR: file %s not found in readAndFilterHalos().", path);
+    }
+    tmp[0] = '\0';
+    for (hrow = 0; hrow < N_HEADER; hrow++) {
+        (void)!fgets(tmp, sizeof(tmp), fp);
+        if (feof(fp)) {
+            fclose(fp);
+            free(filter);
+            return host_fail("ERROR: file %s does not contain headers in readAndFilterHalos().", path);
+        }
+    }
+    fr = 0;
+    for (;;) {
+        sjcs_halo h;
+        (void)!fgets(tmp, sizeof(tmp), fp);
+        if (feof(fp))
+            break;
+        if (parse_record(tmp, &h) < 0) {
+            fclose(fp);
+            free(filter);
+            free(v.h);
+            return host_fail("ERROR: contents in file %s may be incorrect in readAndFilterHalos().", path);
+        }
+        /* An empty filter list reads past its end in the reference; here it
+         * simply keeps nothing. */
+        if (nfilters == 0)
+            break;
+        if (h.id < filter[fr])
+            continue;
+        else if (h.id > filter[fr]) {
+            while (h.id > filter[fr]) {
+                fr++;
+                if (fr >= nfilters) {
+                    finished = 1;
+                    break;
+                }
+            }
+        }
+        if (finished)
+            break;
+        if (h.id == filter[fr] && hv_push(&v, &h) != 0) {
+            fclose(fp);
+            free(filter);
+            free(v.h);
+            return host_fail("ERROR: memory shortage in readAndFilterHalos()");
+        }
+    }
+    fclose(fp);
+    free(filter);
+    *out = v.h ? v.h : malloc(sizeof(sjcs_halo));
+    *n = v.n;
+    return 0;
+}
+
+/* ---- radius schedule ------------------------------------------------------ */
+
+int sjcs_host_radius_table(double minrad, double maxrad, int nrads, float *r2)
+{
+    double a, b, c, t;
+    int i;
+    if (nrads <= 0 || !r2)
+        return host_fail("nrads must be > 0");
+    if (minrad > maxrad) {
+        t = minrad;
+        minrad = maxrad;
+        maxrad = t;
+    }
+    /* Logspace(2, log2(min), log2(max), n) (include/support_functions.h:18-34);
+     * a + i*c is one fused multiply-add in the reference's -march=native build. */
+    a = log2(minrad);
+    b = log2(maxrad);
+    c = (b - a) / (nrads - 1);
+    for (i = 0; i < nrads - 1; ++i)
+        r2[i] = (float)pow(2.0, fma((double)i, c, a));
+    r2[nrads - 1] = (float)pow(2.0, b);
+    for (i = 0; i < nrads; ++i)
+        r2[i] = r2[i] * r2[i];
+    return 0;
+}
+
+/* ---- result text ---------------------------------------------------------- */
+
+static size_t put_u64(char *dst, uint64_t v)
+{
+    char tmp[24];
+    size_t k = 0, i;
+    do {
+        tmp[k++] = (char)('0' + v % 10);
+        v /= 10;
+    } while (v);
+    for (i = 0; i < k; ++i)
+        dst[i] = tmp[k - 1 - i];
+    return k;
+}
+
+typedef struct FmtJob {
+    const sjcs_halo *halos;
+    const uint64_t *counts;
+    uint64_t lo, hi;
+    int nrads;
+    char **labels;
+    size_t *label_len;
+    char *buf;
+    size_t len;
+} FmtJob;
+
+static void *fmt_job(void *arg)
+{
+    FmtJob *j = arg;
+    char *o = j->buf;
+    uint64_t h;
+    int i;
+    for (h = j->lo; h < j->hi; ++h) {
+        const uint64_t *c = j->counts + h * (uint64_t)j->nrads;
+        memcpy(o, "id ", 3);
+        o += 3;
+        o += put_u64(o, j->halos[h].id);
+        *o++ = '\n';
+        for (i = 0; i < j->nrads; ++i) {
+            memcpy(o, j->labels[i], j->label_len[i]);
+            o += j->label_len[i];
+            o += put_u64(o, c[i]);
+            *o++ = '\n';
+        }
+    }
+    j->len = (size_t)(o - j->buf);
+    return NULL;
+}
+
+int sjcs_write_result(const char *path, const sjcs_halo *halos, uint64_t nhalos, const float *r2, int nrads,
+                      const uint64_t *counts, int nthreads)
+{
+    FILE *fp;
+    char **labels = NULL;
+    size_t *label_len = NULL, maxline;
+    float *rad = NULL;
+    uint64_t *total = NULL, h;
+    int i, T, rc = -1;
+    FmtJob *jobs = NULL;
+    pthread_t *th = NULL;
+    const uint64_t per_job = 16384;
+
+    if (nrads <= 0 || !r2)
+        return host_fail("invalid radius table");
+    /* radiuses were squared for the search; print (float)sqrt of them (main.c:386-387) */
+    rad = malloc(nrads * sizeof(float));
+    labels = calloc(nrads, sizeof(char *));
+    label_len = calloc(nrads, sizeof(size_t));
+    total = calloc(nrads, sizeof(uint64_t));
+    if (!rad || !labels || !label_len || !total)
+        goto out;
+    for (i = 0; i < nrads; ++i)
+        rad[i] = (float)sqrt((double)r2[i]);
+    maxline = 0;
+    for (i = 0; i < nrads; ++i) {
+        char b[256];
+        int k = (i == 0) ? snprintf(b, sizeof(b), "  [0.0 ~ %f]: ", rad[0])
+                         : snprintf(b, sizeof(b), "  [%f ~ %f]: ", rad[i - 1], rad[i]);
+        labels[i] = strdup(b);
+        label_len[i] = (size_t)k;
+        if ((size_t)k > maxline)
+            maxline = (size_t)k;
+        if (!labels[i])
+            goto out;
+    }
+    /* Total = sum over all halos, plus halo 0 once more: the reference's
+     * running total is halo 0's own row (main.c:400, 413). */
+    for (h = 0; h < nhalos; ++h)
+        for (i = 0; i < nrads; ++i)
+            total[i] += counts[h * (uint64_t)nrads + i];
+    if (nhalos)
+        for (i = 0; i < nrads; ++i)
+            total[i] += counts[i];
+
+    fp = path ? fopen(path, "w") : stdout;
+    if (!fp) {
+        host_fail("Cannot create %s in outputResult().", path);
+        goto out;
+    }
+    T = default_threads(nthreads);
+    jobs = calloc(T, sizeof(FmtJob));
+    th = calloc(T, sizeof(pthread_t));
+    if (!jobs || !th)
+        goto close_out;
+    for (i = 0; i < T; ++i) {
+        jobs[i].buf = malloc(per_job * (24 + (size_t)nrads * (maxline + 22)));
+        if (!jobs[i].buf)
+            goto close_out;
+    }
+    for (h = 0; h < nhalos;) {
+        int used = 0;
+        for (i = 0; i < T && h < nhalos; ++i) {
+            uint64_t e = h + per_job < nhalos ? h + per_job : nhalos;
+            jobs[i].halos = halos;
+            jobs[i].counts = counts;
+            jobs[i].lo = h;
+            jobs[i].hi = e;
+            jobs[i].nrads = nrads;
+            jobs[i].labels = labels;
+            jobs[i].label_len = label_len;
+            h = e;
+            used++;
+        }
+        for (i = 1; i < used; ++i)
+            pthread_create(&th[i], NULL, fmt_job, &jobs[i]);
+        fmt_job(&jobs[0]);
+        for (i = 1; i < used; ++i)
+            pthread_join(th[i], NULL);
+        for (i = 0; i < used; ++i) {
+            if (fwrite(jobs[i].buf, 1, jobs[i].len, fp) != jobs[i].len) {
+                host_fail("ERROR: while writing %s in outputResult()", path ? path : "(stdout)");
+                goto close_out;
+            }
+        }
+    }
+    fputs("\nTotal\n", fp);
+    for (i = 0; i < nrads; ++i) {
+        char b[32];
+        size_t k = put_u64(b, total[i]);
+        fwrite(labels[i], 1, label_len[i], fp);
+        fwrite(b, 1, k, fp);
+        fputc('\n', fp);
+    }
+    if (ferror(fp)) {
+        host_fail("ERROR: while writing %s in outputResult()", path ? path : "(stdout)");
+        goto close_out;
+    }
+    rc = 0;
+close_out:
+    if (fp != stdout) {
+        if (fclose(fp) != 0 && rc == 0)
+            rc = host_fail("ERROR: while writing %s in outputResult()", path);
+    } else
+        fflush(stdout);
+out:
+    if (jobs)
+        for (i = 0; i < T; ++i)
+            free(jobs[i].buf);
+    free(jobs);
+    free(th);
+    if (labels)
+        for (i = 0; i < nrads; ++i)
+            free(labels[i]);
+    free(labels);
+    free(label_len);
+    free(rad);
+    free(total);
+    return rc;
+}

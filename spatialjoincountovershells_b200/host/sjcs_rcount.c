@@ -1,0 +1,474 @@
+/*
+ * sjcs_rcount -- drop-in for the reference's astr_rcount driver
+ * (src/astr_rcount/main.c), with the index build and the shell count on the
+ * GPU through libsjcs.so.
+ *
+ * Kept from the reference: the command line (same options, same parsing
+ * rules: last occurrence wins, a file list runs to the next argument starting
+ * with '-'), the validation rules and messages (main.c:506-602), the
+ * "--execution info--" block (main.c:604-621), the ">>>> ... time" lines, the
+ * radius schedule (Logspace then squaring, main.c:644-649), counts accumulated
+ * across particle files, and the result text including its Total block
+ * (main.c:371-442).
+ *
+ * Changed: --thread / --next-setup size the host threads that parse the halo
+ * file and format the result (the GPU does the work the thread pool did);
+ * --backlog B keeps up to B particle files read, copied and indexed ahead on
+ * the build stream while the count stream searches the current one (the
+ * reference's backlog pipeline, main.c:266-350, on two CUDA streams); a
+ * missing or unreadable input file is reported and the program exits with
+ * status 1 where the reference dereferences a NULL buffer.
+ */
+#define _GNU_SOURCE
+#include <math.h>
+#include <stdbool.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/time.h>
+
+#include "../../include/sjcs.h"
+#include "../../include/sjcs_host.h"
+
+#define TMP_BUFSIZE 1024
+#define BOOL2STRING(b) ((b) ? "true" : "false")
+
+/* ---- option parsing (src/GetOption/GetOption.c) --------------------------- */
+
+enum { OPT_INT, OPT_STRING_PTR };
+
+static int get_option_value(int argc, char *argv[], void *dst, int type, const char *opt, int offset)
+{
+    size_t optlen = strlen(opt);
+    int i;
+    for (i = 1; i < argc; i++) {
+        if (strlen(argv[i]) != optlen)
+            continue;
+        if (memcmp(argv[i], opt, optlen) == 0) {
+            i += offset + 1;
+            if (i >= argc)
+                return -1;
+            if (type == OPT_INT)
+                *(int *)dst = (int)strtol(argv[i], NULL, 10);
+            else
+                *(char **)dst = argv[i];
+        }
+    }
+    return 0;
+}
+
+static void get_option_range(int argc, char *argv[], int *beg, int *end, const char *opt)
+{
+    size_t optlen = strlen(opt);
+    int i, j;
+    for (i = 1; i < argc; i++) {
+        if (strlen(argv[i]) != optlen)
+            continue;
+        if (memcmp(argv[i], opt, optlen) == 0) {
+            for (j = i + 1; j < argc && *argv[j] != '-'; j++)
+                ;
+            if (j != i + 1) {
+                *beg = i + 1;
+                *end = j;
+            }
+        }
+    }
+}
+
+static bool get_option_flag(int argc, char *argv[], const char *opt)
+{
+    size_t optlen = strlen(opt);
+    int i;
+    for (i = 1; i < argc; i++) {
+        if (strlen(argv[i]) != optlen)
+            continue;
+        if (memcmp(argv[i], opt, optlen) == 0)
+            return true;
+    }
+    return false;
+}
+
+/* ---- timing lines (include/time.h) ---------------------------------------- */
+
+static double now_us(void)
+{
+    struct timeval tv;
+    gettimeofday(&tv, NULL);
+    return tv.tv_sec * 1e6 + tv.tv_usec;
+}
+
+static void print_ms(const char *msg, double t0)
+{
+    long diff = (long)(now_us() - t0);
+    printf("%s: %ld milli seconds\n", msg, diff / 1000);
+}
+
+static void set_error(bool *flag, char *buf, const char *msg)
+{
+    if (!*flag) {
+        *flag = true;
+        strcpy(buf, msg);
+    }
+}
+
+static void usage_exit(char *argv[])
+{
+    fprintf(stderr,
+            "Usage: %s \n"
+            "          --thread #_of_threads_used_in_this_process\n"
+            "          --next-setup #_of_threads_to_build_next_index_in_background\n"
+            "          --particle-files particle_files(1 or more) [--compressed]\n"
+            "          --halo-file halo_file [--filter-file filter_id_list_file]\n"
+            "          --radius minimum_radius:maximum_radius:#_of_bins\n"
+            "          [--backlog max_#_of_backlog_indexes]\n"
+            "          [--first-setup #_of_indexes_be_firstly_built:#_of_threads_to_build_each_index]\n"
+            "          [--output-file output_file_name]\n",
+            argv[0]);
+    exit(EXIT_FAILURE);
+}
+
+static void die_lib(const char *what)
+{
+    fprintf(stderr, "ERROR: %s: %s\n", what, sjcs_last_error());
+    exit(EXIT_FAILURE);
+}
+
+/* ---- one particle file in flight ------------------------------------------ */
+
+typedef struct Pending {
+    int file;
+    float *host;
+    uint64_t n;
+    sjcs_index *idx;
+} Pending;
+
+/* Read a particle file into pinned memory and queue its index build.
+ * Replaces constructIndexWithSameThreadPool (main.c:732-786). */
+static void start_index(sjcs_ctx *ctx, const char *fname, float radius_hint, Pending *p)
+{
+    sjcs_index_opts opts;
+    uint64_t n = 0;
+    double t0;
+    memset(&opts, 0, sizeof(opts));
+    opts.kind = SJCS_INDEX_GRID;
+    opts.radius_hint = radius_hint;
+    t0 = now_us();
+    if (sjcs_particle_file_count(fname, &n) != 0) {
+        fprintf(stderr, "%s\n", sjcs_host_last_error());
+        exit(EXIT_FAILURE);
+    }
+    if (sjcs_host_alloc(n * 3 * sizeof(float), (void **)&p->host) != SJCS_OK)
+        die_lib("pinned buffer");
+    if (sjcs_read_particles(fname, p->host, n, &p->n) != 0) {
+        fprintf(stderr, "%s\n", sjcs_host_last_error());
+        exit(EXIT_FAILURE);
+    }
+    print_ms(">>>> particles reading time", t0);
+    if (sjcs_index_build(ctx, p->host, p->n, &opts, &p->idx) != SJCS_OK)
+        die_lib("index build");
+}
+
+static void finish_index(Pending *p, double t0)
+{
+    if (sjcs_index_wait(p->idx) != SJCS_OK)
+        die_lib("index build");
+    sjcs_host_free(p->host);
+    p->host = NULL;
+    if (t0 >= 0)
+        print_ms(">>>> index construction time", t0);
+    printf("  # of particles = %llu\n", (unsigned long long)p->n);
+}
+
+static void search_and_destroy(sjcs_ctx *ctx, sjcs_query *q, Pending *p)
+{
+    double t0 = now_us();
+    if (sjcs_query_count(ctx, q, p->idx) != SJCS_OK)
+        die_lib("shell count");
+    if (sjcs_ctx_sync(ctx) != SJCS_OK)
+        die_lib("shell count");
+    print_ms(">>>> searching time", t0);
+    t0 = now_us();
+    sjcs_index_destroy(p->idx);
+    p->idx = NULL;
+    print_ms(">>>> index destruction time", t0);
+}
+
+/* noBacklogExecution, main.c:235-264 */
+static void no_backlog(sjcs_ctx *ctx, sjcs_query *q, char **files, int nfiles, float radius_hint)
+{
+    int i;
+    puts("  -- with no backlog execution");
+    for (i = 0; i < nfiles; i++) {
+        Pending p;
+        double t0;
+        memset(&p, 0, sizeof(p));
+        p.file = i;
+        start_index(ctx, files[i], radius_hint, &p);
+        t0 = now_us();
+        finish_index(&p, t0);
+        search_and_destroy(ctx, q, &p);
+    }
+}
+
+/* withBacklogExecution, main.c:266-350: up to maxbacklogs files are read and
+ * indexed ahead (first_nbacklogs of them before the first search); each
+ * search overlaps the reading and building of the files behind it. */
+static void with_backlog(sjcs_ctx *ctx, sjcs_query *q, char **files, int nfiles, int maxbacklogs,
+                         int first_nbacklogs, float radius_hint)
+{
+    Pending *ring = calloc((size_t)maxbacklogs + 1, sizeof(Pending));
+    int head = 0, count = 0, next = 0, i, cap = maxbacklogs + 1;
+    puts("  -- with backlog execution");
+    while (count < first_nbacklogs && next < nfiles) {
+        Pending *p = &ring[(head + count) % cap];
+        memset(p, 0, sizeof(*p));
+        p->file = next;
+        printf("index %d\n", next);
+        start_index(ctx, files[next], radius_hint, p);
+        next++;
+        count++;
+    }
+    for (i = 0; i < nfiles; i++) {
+        Pending *cur;
+        double t0;
+        if (count == 0) { /* nothing ahead: build it now */
+            Pending *p = &ring[head];
+            memset(p, 0, sizeof(*p));
+            p->file = next;
+            printf("index %d\n", next);
+            start_index(ctx, files[next], radius_hint, p);
+            next++;
+            count++;
+        }
+        cur = &ring[head];
+        t0 = now_us();
+        finish_index(cur, -1.0);
+        print_ms(">>>> index getting time", t0);
+        head = (head + 1) % cap;
+        count--;
+        t0 = now_us();
+        if (sjcs_query_count(ctx, q, cur->idx) != SJCS_OK)
+            die_lib("shell count");
+        /* read and queue the next files while the search runs */
+        while (count < maxbacklogs && next < nfiles) {
+            Pending *p = &ring[(head + count) % cap];
+            memset(p, 0, sizeof(*p));
+            p->file = next;
+            printf("index %d\n", next);
+            start_index(ctx, files[next], radius_hint, p);
+            next++;
+            count++;
+        }
+        /* wait for this file's search only; the builds queued behind it keep running */
+        if (sjcs_query_wait(q) != SJCS_OK)
+            die_lib("shell count");
+        print_ms(">>>> searching time", t0);
+        t0 = now_us();
+        sjcs_index_destroy(cur->idx);
+        cur->idx = NULL;
+        print_ms(">>>> index destruction time", t0);
+    }
+    free(ring);
+}
+
+int main(int argc, char *argv[])
+{
+    char *outfile_name = NULL;
+    int particle_beg = -1, particle_end = -1;
+    bool particle_compressed;
+    char *halo_name = NULL, *halo_filter_name = NULL;
+    int nrads = 0;
+    double minrad = 0.0, maxrad = 0.0;
+    char *range_str = NULL;
+    int maxbacklogs = 0, nthreads = -1, nsetups = -1;
+    int first_nbacklogs = 1, first_nsetups = 1;
+    char *setup_str = NULL;
+    bool errflag = false;
+    char errmsg[TMP_BUFSIZE];
+    int i;
+    sjcs_halo *halos = NULL;
+    uint64_t nhalos = 0;
+    float *r2;
+    uint64_t *counts;
+    sjcs_ctx *ctx = NULL;
+    sjcs_query *q = NULL;
+    double t0, t_total;
+
+    /*** argument processing (main.c:492-602) ***/
+    get_option_value(argc, argv, &outfile_name, OPT_STRING_PTR, "--output-file", 0);
+    get_option_range(argc, argv, &particle_beg, &particle_end, "--particle-files");
+    particle_compressed = get_option_flag(argc, argv, "--compressed");
+    get_option_value(argc, argv, &halo_name, OPT_STRING_PTR, "--halo-file", 0);
+    get_option_value(argc, argv, &halo_filter_name, OPT_STRING_PTR, "--filter-file", 0);
+
+    get_option_value(argc, argv, &range_str, OPT_STRING_PTR, "--radius", 0);
+    if (range_str != NULL) {
+        char *delimp;
+        minrad = strtod(range_str, NULL);
+        if ((delimp = strchr(range_str, ':')) != NULL) {
+            maxrad = strtod(delimp + 1, NULL);
+            if ((delimp = strrchr(range_str, ':')) != NULL)
+                nrads = (int)strtol(delimp + 1, NULL, 10);
+        }
+    }
+    if (range_str == NULL || nrads <= 0 || minrad <= 0 || maxrad <= 0) {
+        set_error(&errflag, errmsg,
+                  "# of ranges, minimum range, maximum range must be > 0.\n"
+                  "      use --radius and fix.\n");
+    } else if (minrad == maxrad) {
+        set_error(&errflag, errmsg,
+                  "minimum range must be <  maximum range.\n"
+                  "      use --radius and fix.\n");
+    }
+    if (minrad > maxrad) {
+        double t = minrad;
+        minrad = maxrad;
+        maxrad = t;
+    }
+
+    get_option_value(argc, argv, &maxbacklogs, OPT_INT, "--backlog", 0);
+    if (maxbacklogs < 0) {
+        set_error(&errflag, errmsg,
+                  "max # of backlog indexes must be >= 0.\n"
+                  "      use --backlog and fix.\n");
+    }
+    get_option_value(argc, argv, &nthreads, OPT_INT, "--thread", 0);
+    get_option_value(argc, argv, &nsetups, OPT_INT, "--next-setup", 0);
+    if (nthreads < 1) {
+        set_error(&errflag, errmsg,
+                  "# of threads must be >= 1.\n"
+                  "      use --thread and fix.\n");
+    }
+    if (nsetups < 1) {
+        set_error(&errflag, errmsg,
+                  "# of backlog index construction threads must be >= 1.\n"
+                  "      use --next-setup and fix.\n");
+    }
+    get_option_value(argc, argv, &setup_str, OPT_STRING_PTR, "--first-setup", 0);
+    if (setup_str != NULL) {
+        char *delimp;
+        first_nbacklogs = (int)strtol(setup_str, NULL, 10);
+        if ((delimp = strchr(setup_str, ':')) != NULL)
+            first_nsetups = (int)strtol(delimp + 1, NULL, 10);
+    }
+    if (maxbacklogs == 0) {
+        if (nthreads < nsetups) {
+            set_error(&errflag, errmsg,
+                      "in noBacklogExecution; # of threads must be"
+                      ">= # of index construction threads.\n"
+                      "      use --thread, --next-setup and fix.\n");
+        }
+    } else {
+        if ((nthreads < (nsetups + 1) || nthreads < (first_nsetups + 1))) {
+            set_error(&errflag, errmsg,
+                      "in withBacklogExecution; # of threads must be"
+                      "> # of index construction threads.\n"
+                      "      use --thread, --next-setup, --first-setup and fix.\n");
+        }
+        if (maxbacklogs < first_nbacklogs) {
+            set_error(&errflag, errmsg,
+                      "in withBacklogExecution; max # of backlog indexes must be"
+                      "> # of first backlog indexes.\n"
+                      "      use --backlog, --first-setup and fix.\n");
+        }
+    }
+    if (particle_beg <= 0) {
+        set_error(&errflag, errmsg,
+                  "particle file is missing.\n"
+                  "      use --particle-files and fix.\n");
+    }
+    if (halo_name == NULL) {
+        set_error(&errflag, errmsg,
+                  "halo file is missing.\n"
+                  "      use --halo-file and fix.\n");
+    }
+
+    puts("\n--execution info--");
+    printf("  particle files (compressed = %s): \n", BOOL2STRING(particle_compressed));
+    for (i = particle_beg; i < particle_end; i++)
+        printf("   |- %s\n", argv[i]);
+    printf("  halo file = %s\n"
+           "  halo filter file = %s\n"
+           "  # of threads in thread pool = %d\n"
+           "  # of index construction threads = %d\n"
+           "  # of radiuses = %d\n"
+           "   |- minimum = %f, maximum = %f\n"
+           "  max # of backlog indexes = %d\n"
+           "  %s# of first backlog indexes = %d\n"
+           "  %s# of first index construction threads = %d\n",
+           halo_name ? halo_name : "(null)", halo_filter_name ? halo_filter_name : "(null)", nthreads, nsetups,
+           nrads, minrad, maxrad, maxbacklogs, (maxbacklogs == 0) ? "! ignored ! " : "", first_nbacklogs,
+           (maxbacklogs == 0) ? "! ignored ! " : "", first_nsetups);
+    fflush(stdout);
+
+    if (errflag) {
+        fprintf(stderr, "\n => %s\n", errmsg);
+        usage_exit(argv);
+    }
+    if (particle_compressed) {
+        fprintf(stderr, "ERROR: --compressed (Gadget-encoded) particle files are not supported by this build.\n");
+        exit(EXIT_FAILURE);
+    }
+
+    /*** initialize ***/
+    if (sjcs_ctx_create(0, &ctx) != SJCS_OK)
+        die_lib("GPU context");
+
+    t0 = now_us();
+    if (halo_filter_name == NULL) {
+        if (sjcs_read_halos(halo_name, &halos, &nhalos, nthreads) != 0) {
+            fprintf(stderr, "%s\n", sjcs_host_last_error());
+            exit(EXIT_FAILURE);
+        }
+    } else {
+        if (sjcs_read_and_filter_halos(halo_name, halo_filter_name, &halos, &nhalos) != 0) {
+            fprintf(stderr, "%s\n", sjcs_host_last_error());
+            exit(EXIT_FAILURE);
+        }
+    }
+    print_ms(">>>> halo data reading time", t0);
+    printf("  # of halos = %lu\n", (unsigned long)nhalos);
+
+    r2 = malloc(sizeof(float) * nrads);
+    if (sjcs_radius_table(minrad, maxrad, nrads, r2) != SJCS_OK)
+        die_lib("radius table");
+    counts = calloc(1, sizeof(uint64_t) * (size_t)nrads * (nhalos ? nhalos : 1));
+    if (!r2 || !counts) {
+        fprintf(stderr, "ERROR: memory shortage\n");
+        exit(EXIT_FAILURE);
+    }
+    if (sjcs_query_create(ctx, nhalos ? halos[0].point : NULL, sizeof(sjcs_halo), nhalos, r2, nrads,
+                          SJCS_QUERY_PERIODIC, &q) != SJCS_OK)
+        die_lib("halo upload");
+
+    /*** execution ***/
+    t_total = now_us();
+    {
+        const float radius_hint = (float)sqrt((double)r2[nrads - 1]);
+        char **files = &argv[particle_beg];
+        const int nfiles = particle_end - particle_beg;
+        if (maxbacklogs == 0)
+            no_backlog(ctx, q, files, nfiles, radius_hint);
+        else
+            with_backlog(ctx, q, files, nfiles, maxbacklogs, first_nbacklogs, radius_hint);
+    }
+    if (sjcs_query_read_counts(ctx, q, counts, 1) != SJCS_OK)
+        die_lib("count read-back");
+    print_ms(">>>> total searching time", t_total);
+
+    /*** result processing ***/
+    t0 = now_us();
+    fflush(stdout);
+    if (sjcs_write_result(outfile_name, halos, nhalos, r2, nrads, counts, nthreads) != 0) {
+        fprintf(stderr, "%s\n", sjcs_host_last_error());
+        exit(EXIT_FAILURE);
+    }
+    print_ms(">>>> result writing time", t0);
+
+    sjcs_query_destroy(q);
+    sjcs_ctx_destroy(ctx);
+    sjcs_host_free_halos(halos);
+    free(r2);
+    free(counts);
+    return 0;
+}

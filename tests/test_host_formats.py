@@ -1,0 +1,148 @@
+"""Host-side formats: generators, readers and the result writer (CPU only)."""
+from __future__ import annotations
+
+import hashlib
+
+import numpy as np
+import pytest
+
+from conftest import golden_counts
+from golden import cases
+from oracle import oracle
+from spatialjoincountovershells_b200 import _native as nat
+
+needs_ref = pytest.mark.skipif(not oracle.ref_available(), reason="reference binaries not built")
+
+
+@needs_ref
+def test_particle_generator_matches_reference(tmp_path, built):
+    r = oracle.run_ref(["-f", "a.dat", "b.dat", "-n", "5000", "-s", "17"], exe=oracle.REF_PGEN, cwd=tmp_path)
+    assert r.returncode == 0
+    ref = np.concatenate([np.fromfile(tmp_path / "a.dat", np.float32), np.fromfile(tmp_path / "b.dat", np.float32)])
+    ours = nat.gen_uniform_particles(17, 2, 5000).reshape(-1)
+    assert np.array_equal(ref.view(np.uint32), ours.view(np.uint32))
+
+
+@needs_ref
+def test_halo_generator_matches_reference(tmp_path, built):
+    r = oracle.run_ref(["-f", "h.list", "-n", "3000", "-s", "23"], exe=oracle.REF_HGEN, cwd=tmp_path)
+    assert r.returncode == 0
+    nat.gen_uniform_halo_file(tmp_path / "mine.list", 23, 3000)
+    assert (tmp_path / "h.list").read_bytes() == (tmp_path / "mine.list").read_bytes()
+
+
+def test_generator_checksums_pinned(tmp_path, built):
+    # pins the generators where the reference binaries are absent
+    p = nat.gen_uniform_particles(1, 1, 1000)
+    assert hashlib.sha256(p.tobytes()).hexdigest()[:16] == _PIN_PARTICLES
+    nat.gen_uniform_halo_file(tmp_path / "h.list", 2, 500)
+    assert hashlib.sha256((tmp_path / "h.list").read_bytes()).hexdigest()[:16] == _PIN_HALOS
+
+
+_PIN_PARTICLES = "35967606d4eb08e1"  # sha256 prefix, uniform_decoded_particle_generator -n 1000 -s 1
+_PIN_HALOS = "27c0f3b7ccdfbbb6"  # sha256 prefix, uniform_halo_generator -n 500 -s 2
+
+
+def test_in_memory_halos_equal_parsed_file(tmp_path, built):
+    nat.gen_uniform_halo_file(tmp_path / "h.list", 29, 4000, 10)
+    parsed = nat.read_halos(tmp_path / "h.list")
+    mem = nat.gen_uniform_halos(29, 4000, 10)
+    assert parsed.tobytes() == mem.tobytes()
+    face = nat.gen_face_halos(3, 300, 0, margin=5.0)
+    nat.write_halo_file(tmp_path / "f.list", face)
+    assert nat.read_halos(tmp_path / "f.list").tobytes() == face.tobytes()
+
+
+def _halo_text(lines, header=16):
+    return "".join(f"# dummy header {k}\n" for k in range(header)) + "".join(lines)
+
+
+REC = "7 0 1.5e+11 0 0 0 0 0 1.5 2.5 3.5 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0 0\n"
+
+
+def test_halo_reader_acceptance_rules(tmp_path, built):
+    f = tmp_path / "h.list"
+    # a last line without a newline is ignored (fgets reaches end of file)
+    f.write_text(_halo_text([REC, REC.rstrip("\n")]))
+    h = nat.read_halos(f)
+    assert len(h) == 1 and h[0]["id"] == 7 and tuple(h[0]["point"]) == (1.5, 2.5, 3.5)
+    assert h[0]["mass"] == np.float32(1.5e11)
+    # fewer than 16 header lines
+    f.write_text(_halo_text([], header=15))
+    with pytest.raises(nat.SjcsError, match="does not contain headers"):
+        nat.read_halos(f)
+    # 16th header line without newline also counts as missing
+    f.write_text(_halo_text([], header=15) + "# dummy header 15")
+    with pytest.raises(nat.SjcsError, match="does not contain headers"):
+        nat.read_halos(f)
+    # exactly 16 header lines and nothing else: zero halos
+    f.write_text(_halo_text([]))
+    assert len(nat.read_halos(f)) == 0
+    # a record with too few fields
+    f.write_text(_halo_text([REC, "1 2 3\n"]))
+    with pytest.raises(nat.SjcsError, match="may be incorrect"):
+        nat.read_halos(f)
+    # an empty line is a bad record too
+    f.write_text(_halo_text([REC, "\n", REC]))
+    with pytest.raises(nat.SjcsError, match="may be incorrect"):
+        nat.read_halos(f)
+    with pytest.raises(nat.SjcsError, match="not found"):
+        nat.read_halos(tmp_path / "missing.list")
+
+
+def test_halo_reader_long_lines_split_like_fgets(tmp_path, built):
+    # A line longer than the reference's 16 KiB fgets buffer is read as several
+    # records; the reader falls back to the literal fgets loop for such files.
+    f = tmp_path / "h.list"
+    long_rec = REC.rstrip("\n") + " 0" * 9000 + "\n"
+    f.write_text(_halo_text([REC, long_rec, REC]))
+    h = nat.read_halos(f)
+    # long record: first piece parses as a halo; the remaining pieces are "0 0 0 ..." records
+    pieces = -(-len(long_rec) // 16383)
+    assert len(h) == 2 + pieces
+    assert h[0]["id"] == 7 and h[1]["id"] == 7 and h[-1]["id"] == 7
+
+
+def test_halo_reader_parallel_equals_serial(tmp_path, built):
+    nat.gen_uniform_halo_file(tmp_path / "h.list", 31, 50000)
+    a = nat.read_halos(tmp_path / "h.list", nthreads=1)
+    b = nat.read_halos(tmp_path / "h.list", nthreads=8)
+    assert a.tobytes() == b.tobytes() and len(a) == 50000
+
+
+def test_filter_reader_intended_merge_join(tmp_path, built):
+    # The reference never stores the filter count (ConstructFilterIdList,
+    # src/Gadget/BufHalo.c:132-180), so its result depends on heap contents.
+    # The reader implements the evident intent: sort the ids, keep every halo
+    # whose id is listed (halo ids ascending, as the merge-join assumes).
+    nat.gen_uniform_halo_file(tmp_path / "h.list", 14, 200)
+    (tmp_path / "f.txt").write_text("150\n5\n7\n7\n100\n3\n199\n1000")
+    h = nat.read_halos(tmp_path / "h.list", filter_path=tmp_path / "f.txt")
+    assert list(h["id"]) == [3, 5, 7, 100, 150, 199]
+    allh = nat.read_halos(tmp_path / "h.list")
+    assert h.tobytes() == allh[[3, 5, 7, 100, 150, 199]].tobytes()
+
+
+def test_particle_reader(tmp_path, built):
+    p = nat.gen_uniform_particles(3, 1, 777)
+    nat.write_particle_file(tmp_path / "p.dat", p)
+    with open(tmp_path / "p.dat", "ab") as fh:  # trailing partial record is ignored (size / 12)
+        fh.write(b"\x00" * 7)
+    q = nat.read_particles(tmp_path / "p.dat")
+    assert np.array_equal(p, q)
+    with pytest.raises(nat.SjcsError, match="not found"):
+        nat.read_particles(tmp_path / "nope.dat")
+
+
+@pytest.mark.parametrize("name", list(cases.CASES))
+def test_result_writer_reproduces_reference_text(name, case_dirs, manifest, tmp_path):
+    d, spec = case_dirs[name]
+    halos, _ = cases.load_halos_and_particles(spec, d)
+    ids, counts, _ = golden_counts(name)
+    r2 = nat.radius_table(*cases.radius_spec(spec))
+    out = tmp_path / "r.txt"
+    nat.write_result(out, halos, r2, counts, nthreads=3)
+    data = out.read_bytes()
+    assert hashlib.sha256(data).hexdigest() == manifest[name]["sha256"]
+    if name == "kat":
+        assert data == (cases.pathlib.Path(__file__).parent / "golden" / "kat_result.txt").read_bytes()
