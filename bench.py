@@ -323,9 +323,12 @@ def run_ours(args, w, dist, rank, world, local):
 
     K, W = args.steps, args.warmup
     ms, launches, count_ms, clocks = timed(step_resident, K, W, keep_queries=True)
-    ms_e2e, launches_e2e, _, clocks_e2e = timed(step_e2e, K, W, keep_queries=False)
     ms = dist_max(dist, ms, local)
-    ms_e2e = dist_max(dist, ms_e2e, local)
+    if args.no_e2e:
+        ms_e2e, launches_e2e, clocks_e2e = float("nan"), 0, None
+    else:
+        ms_e2e, launches_e2e, _, clocks_e2e = timed(step_e2e, K, W, keep_queries=False)
+        ms_e2e = dist_max(dist, ms_e2e, local)
 
     # one extra untimed pass for the per-phase split (build vs search)
     q = ctx.query(halos_d, r2)
@@ -340,7 +343,7 @@ def run_ours(args, w, dist, rank, world, local):
     q.destroy()
     # correctness spot-check of the timed path on a halo sample (oracle, file 0)
     check = None
-    if rank == 0 and not args.no_check:
+    if rank == 0 and not args.no_check and not args.no_e2e:
         from oracle import oracle
         sample = 2000
         got = out_np[:sample]
@@ -377,9 +380,10 @@ def run_ours(args, w, dist, rank, world, local):
                    "l2": "inputs larger than L2 (3 x 1.2 GB particle arrays per step)"},
         "build_s_per_file": round(statistics.mean(bt) / 1e3, 5),
         "search_halos_per_s": round(nh * nf / (qt["count_ms"] / 1e3), 1) if qt["count_ms"] else None,
-        "e2e": {"value": round(e2e_value, 1), "unit": UNIT, "ms_per_step": round(ms_e2e, 3),
-                "h2d_bytes_per_step": int(nf * n * 12 + (nh - 1) * 24 + 12),
-                "d2h_bytes_per_step": int(nh * nr * 8)},
+        "e2e": None if args.no_e2e else {
+            "value": round(e2e_value, 1), "unit": UNIT, "ms_per_step": round(ms_e2e, 3),
+            "h2d_bytes_per_step": int(nf * n * 12 + (nh - 1) * 24 + 12),
+            "d2h_bytes_per_step": int(nh * nr * 8)},
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": clocks,
@@ -463,12 +467,19 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--small", action="store_true", help="a 50x smaller workload (smoke runs, CPU tests)")
+    ap.add_argument("--files", type=int, default=None, help="override the number of particle files")
+    ap.add_argument("--halos", type=int, default=None, help="override the number of halos (same density)")
+    ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    w = SMALL if args.small else FULL
+    w = dict(SMALL if args.small else FULL)
+    if args.files:
+        w["nfiles"] = args.files
+    if args.halos:
+        w["nhalos"] = args.halos
     if args.impl == "reference":
         # the reference is a CPU program: rank 0 alone runs it, other ranks exit
         if int(os.environ.get("RANK", "0")) != 0:

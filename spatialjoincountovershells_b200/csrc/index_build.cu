@@ -8,9 +8,9 @@
 // hull of its children (adjustMbrArraySTRNode, src/objects/ArraySTR/Node.c:10-58)
 // -- so any index that returns a superset of the in-box points gives the same
 // counts.  Here the index is a uniform cell grid:
-//   pass 0   key = cell of (x,y,z), computed from the AoS input on the fly
-//   passes   stable LSD radix sort of (key, particle id), 8 bits per pass
-//   last     the final scatter gathers x,y,z into sorted SoA arrays
+//   pass 0   key = cell of (x,y,z) and payload = (x,y,z), read from the AoS input
+//   passes   stable LSD radix sort of (key, payload), 8 bits per pass
+//   last     writes the sorted particles as float4 and the sorted keys
 //   offsets  cell_start[c] = first sorted slot of cell c (boundary fill)
 #include <algorithm>
 #include <cmath>
@@ -28,20 +28,20 @@ struct KeysFromParticles {
         return cell_key(g, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
     }
 };
-
-// Last pass: write the sorted key and gather the particle into SoA slot g.
-struct SinkGatherParticles {
+struct PayFromParticles {
     const float* __restrict__ xyz;
+    __device__ __forceinline__ uint4 operator()(uint64_t i) const {
+        return make_uint4(__float_as_uint(xyz[3 * i]), __float_as_uint(xyz[3 * i + 1]),
+                          __float_as_uint(xyz[3 * i + 2]), 0u);
+    }
+};
+// Last pass: sorted key (for the offsets) and the particle as float4.
+struct SinkParticles {
     uint32_t* __restrict__ keys;
-    float* __restrict__ xs;
-    float* __restrict__ ys;
-    float* __restrict__ zs;
-    __device__ __forceinline__ void operator()(uint32_t g, uint32_t k, uint32_t v) const {
+    uint4* __restrict__ pts;
+    __device__ __forceinline__ void operator()(uint32_t g, uint32_t k, const uint4& v) const {
         keys[g] = k;
-        const uint64_t s = 3ull * v;
-        xs[g] = xyz[s];
-        ys[g] = xyz[s + 1];
-        zs[g] = xyz[s + 2];
+        pts[g] = v;
     }
 };
 
@@ -122,75 +122,43 @@ int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGe
     (void)ctx;
     idx->geom = g;
     const uint64_t nalloc = n ? n : 1;
-    SJCS_CUDA_TRY(cudaMallocAsync(&idx->xs, nalloc * sizeof(float), s));
-    SJCS_CUDA_TRY(cudaMallocAsync(&idx->ys, nalloc * sizeof(float), s));
-    SJCS_CUDA_TRY(cudaMallocAsync(&idx->zs, nalloc * sizeof(float), s));
+    SJCS_CUDA_TRY(cudaMallocAsync(&idx->pts, nalloc * sizeof(float4), s));
     SJCS_CUDA_TRY(cudaMallocAsync(&idx->cell_start, (g.ncells + 1) * sizeof(uint32_t), s));
 
-    uint32_t *ka = nullptr, *kb = nullptr, *va = nullptr, *vb = nullptr, *hist = nullptr;
+    uint32_t *kx = nullptr, *ky = nullptr, *kfinal = nullptr, *hist = nullptr;
+    uint4* px = nullptr;
+    uint4* py = nullptr;
     Gap* gaps = nullptr;
     uint32_t* ngaps = nullptr;
     const uint32_t max_gaps = 1u << 16;
-    const uint64_t ntiles64 = (n + RS_TILE - 1) / RS_TILE;
-    const uint32_t ntiles = (uint32_t)ntiles64;
+    const uint64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
+    int key_bits = 1;
+    while (key_bits < 32 && (1ull << key_bits) < g.ncells) ++key_bits;
+    const int passes = (key_bits + RS_BITS - 1) / RS_BITS;
     StreamScratch scr(s);  // freed (stream-ordered) on every return path
-    SJCS_CUDA_TRY(scr.alloc(&ka, nalloc * sizeof(uint32_t)));
-    SJCS_CUDA_TRY(scr.alloc(&kb, nalloc * sizeof(uint32_t)));
-    SJCS_CUDA_TRY(scr.alloc(&va, nalloc * sizeof(uint32_t)));
-    SJCS_CUDA_TRY(scr.alloc(&vb, nalloc * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&kfinal, nalloc * sizeof(uint32_t)));
+    if (passes > 1) {
+        SJCS_CUDA_TRY(scr.alloc(&kx, nalloc * sizeof(uint32_t)));
+        SJCS_CUDA_TRY(scr.alloc(&px, nalloc * sizeof(uint4)));
+    }
+    if (passes > 2) {
+        SJCS_CUDA_TRY(scr.alloc(&ky, nalloc * sizeof(uint32_t)));
+        SJCS_CUDA_TRY(scr.alloc(&py, nalloc * sizeof(uint4)));
+    }
     SJCS_CUDA_TRY(scr.alloc(&hist, ((uint64_t)RS_BINS * (ntiles ? ntiles : 1)) * sizeof(uint32_t)));
     SJCS_CUDA_TRY(scr.alloc(&gaps, max_gaps * sizeof(Gap)));
     SJCS_CUDA_TRY(scr.alloc(&ngaps, sizeof(uint32_t)));
     SJCS_CUDA_TRY(cudaMemsetAsync(ngaps, 0, sizeof(uint32_t), s));
 
-    uint32_t* sorted_keys = ka;
-    if (n > 0) {
-        int key_bits = 1;
-        while (key_bits < 32 && (1ull << key_bits) < g.ncells) ++key_bits;
-        const int passes = (key_bits + RS_BITS - 1) / RS_BITS;
-        const KeysFromParticles kp{d_xyz, g};
-        uint32_t *kin = nullptr, *vin = nullptr, *kout = ka, *vout = va;
-        for (int p = 0; p < passes; ++p) {
-            const int shift = p * RS_BITS;
-            const bool first = (p == 0), last = (p == passes - 1);
-            if (first)
-                k_radix_upsweep<<<ntiles, RS_THREADS, 0, s>>>(kp, n, shift, hist, ntiles);
-            else
-                k_radix_upsweep<<<ntiles, RS_THREADS, 0, s>>>(KeysFromArray{kin}, n, shift, hist, ntiles);
-            SJCS_LAUNCH_CHECK();
-            int rc = exclusive_scan_u32(hist, (uint64_t)RS_BINS * ntiles, s);
-            if (rc) return rc;
-            if (last) {
-                const SinkGatherParticles sink{d_xyz, kout, idx->xs, idx->ys, idx->zs};
-                if (first)
-                    k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(kp, ValsIota{}, n, shift, hist, ntiles, sink);
-                else
-                    k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(KeysFromArray{kin}, ValsFromArray{vin}, n,
-                                                                     shift, hist, ntiles, sink);
-            } else {
-                const SinkPairs sink{kout, vout};
-                if (first)
-                    k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(kp, ValsIota{}, n, shift, hist, ntiles, sink);
-                else
-                    k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(KeysFromArray{kin}, ValsFromArray{vin}, n,
-                                                                     shift, hist, ntiles, sink);
-            }
-            SJCS_LAUNCH_CHECK();
-            sorted_keys = kout;
-            kin = kout;
-            vin = vout;
-            kout = (kout == ka) ? kb : ka;
-            vout = (vout == va) ? vb : va;
-        }
-    }
-    {
-        const uint64_t threads = n + 1;
-        const unsigned blocks = (unsigned)((threads + 255) / 256);
-        k_cell_start<<<blocks, 256, 0, s>>>(sorted_keys, n, g.ncells, idx->cell_start, gaps, ngaps, max_gaps);
-        SJCS_LAUNCH_CHECK();
-        k_fill_gaps<<<1024, 256, 0, s>>>(gaps, ngaps, max_gaps, idx->cell_start);
-        SJCS_LAUNCH_CHECK();
-    }
+    int rc = radix_sort_records(n, key_bits, KeysFromParticles{d_xyz, g}, PayFromParticles{d_xyz},
+                                SinkParticles{kfinal, reinterpret_cast<uint4*>(idx->pts)}, kx, px, ky, py, hist, s);
+    if (rc) return rc;
+    const uint64_t threads = n + 1;
+    const unsigned blocks = (unsigned)((threads + 255) / 256);
+    k_cell_start<<<blocks, 256, 0, s>>>(kfinal, n, g.ncells, idx->cell_start, gaps, ngaps, max_gaps);
+    SJCS_LAUNCH_CHECK();
+    k_fill_gaps<<<1024, 256, 0, s>>>(gaps, ngaps, max_gaps, idx->cell_start);
+    SJCS_LAUNCH_CHECK();
     return SJCS_OK;
 }
 

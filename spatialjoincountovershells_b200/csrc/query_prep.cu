@@ -23,14 +23,19 @@ struct KeysFromHalos {
     }
 };
 
-struct SinkHalos {
+// payload: x, y, z and the halo's index in the caller's order
+struct PayFromHalos {
     const char* __restrict__ base;
     size_t stride;
-    float4* __restrict__ out;
-    __device__ __forceinline__ void operator()(uint32_t g, uint32_t, uint32_t v) const {
-        const float3 h = load_halo(base, stride, v);
-        out[g] = make_float4(h.x, h.y, h.z, __uint_as_float(v));
+    __device__ __forceinline__ uint4 operator()(uint64_t i) const {
+        const float3 h = load_halo(base, stride, i);
+        return make_uint4(__float_as_uint(h.x), __float_as_uint(h.y), __float_as_uint(h.z), (uint32_t)i);
     }
+};
+
+struct SinkHalos {
+    uint4* __restrict__ out;
+    __device__ __forceinline__ void operator()(uint32_t g, uint32_t, const uint4& v) const { out[g] = v; }
 };
 
 }  // namespace
@@ -40,47 +45,17 @@ int sort_halos(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride_bytes, uint
     (void)ctx;
     if (nhalos == 0) return SJCS_OK;
     const char* base = reinterpret_cast<const char*>(d_halo_xyz);
-    const uint32_t ntiles = (uint32_t)((nhalos + RS_TILE - 1) / RS_TILE);
-    uint32_t *ka, *kb, *va, *vb, *hist;
+    const uint64_t ntiles = (nhalos + RS_TILE - 1) / RS_TILE;
+    uint32_t *kx, *ky, *hist;
+    uint4 *px, *py;
     StreamScratch scr(s);
-    SJCS_CUDA_TRY(scr.alloc(&ka, nhalos * sizeof(uint32_t)));
-    SJCS_CUDA_TRY(scr.alloc(&kb, nhalos * sizeof(uint32_t)));
-    SJCS_CUDA_TRY(scr.alloc(&va, nhalos * sizeof(uint32_t)));
-    SJCS_CUDA_TRY(scr.alloc(&vb, nhalos * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&kx, nhalos * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&ky, nhalos * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&px, nhalos * sizeof(uint4)));
+    SJCS_CUDA_TRY(scr.alloc(&py, nhalos * sizeof(uint4)));
     SJCS_CUDA_TRY(scr.alloc(&hist, (uint64_t)RS_BINS * ntiles * sizeof(uint32_t)));
-    const KeysFromHalos kh{base, stride_bytes};
-    const int passes = 4;  // 30-bit keys
-    uint32_t *kin = nullptr, *vin = nullptr, *kout = ka, *vout = va;
-    for (int p = 0; p < passes; ++p) {
-        const int shift = p * RS_BITS;
-        const bool first = (p == 0), last = (p == passes - 1);
-        if (first)
-            k_radix_upsweep<<<ntiles, RS_THREADS, 0, s>>>(kh, nhalos, shift, hist, ntiles);
-        else
-            k_radix_upsweep<<<ntiles, RS_THREADS, 0, s>>>(KeysFromArray{kin}, nhalos, shift, hist, ntiles);
-        SJCS_LAUNCH_CHECK();
-        int rc = exclusive_scan_u32(hist, (uint64_t)RS_BINS * ntiles, s);
-        if (rc) return rc;
-        if (last) {
-            const SinkHalos sink{base, stride_bytes, out};
-            k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(KeysFromArray{kin}, ValsFromArray{vin}, nhalos,
-                                                             shift, hist, ntiles, sink);
-        } else {
-            const SinkPairs sink{kout, vout};
-            if (first)
-                k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(kh, ValsIota{}, nhalos, shift, hist, ntiles,
-                                                                 sink);
-            else
-                k_radix_downsweep<<<ntiles, RS_THREADS, 0, s>>>(KeysFromArray{kin}, ValsFromArray{vin}, nhalos,
-                                                                 shift, hist, ntiles, sink);
-        }
-        SJCS_LAUNCH_CHECK();
-        kin = kout;
-        vin = vout;
-        kout = (kout == ka) ? kb : ka;
-        vout = (vout == va) ? vb : va;
-    }
-    return SJCS_OK;
+    return radix_sort_records(nhalos, 30, KeysFromHalos{base, stride_bytes}, PayFromHalos{base, stride_bytes},
+                              SinkHalos{reinterpret_cast<uint4*>(out)}, kx, px, ky, py, hist, s);
 }
 
 }  // namespace sjcs

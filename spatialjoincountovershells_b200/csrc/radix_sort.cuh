@@ -1,34 +1,38 @@
-// Stable LSD radix sort of (u32 key, u32 value) pairs, 8-bit digits,
+// Stable LSD radix sort of (u32 key, 16-byte payload) records, 8-bit digits,
 // reduce-then-scan per digit pass:
 //   k_radix_upsweep    per-tile digit histogram           -> hist[digit][tile]
 //   exclusive_scan_u32 over hist (digit-major)            -> global slot base of (digit, tile)
-//   k_radix_downsweep  stable in-tile rank (warp match),   shared-memory exchange so that
-//                      each digit run leaves as consecutive (coalesced) stores
-// No block ever waits on another block.
+//   k_radix_downsweep  stable in-tile rank (warp match),   shared-memory exchange of key and
+//                      payload so each digit run leaves as consecutive (coalesced) stores
+// No block ever waits on another block.  The payload travels with the key
+// through every pass, so no pass reads memory at random.
 //
 // The reference sorts with 8-bit LSD passes too (Build.c:164-201, 407-534:
 // per-thread 256-bin histograms, prefix sums, 32-entry local buffers); here a
-// tile of 4096 keys plays the role of a thread's slice and the shared-memory
+// tile of 4096 records plays the role of a thread's slice and the shared-memory
 // exchange plays the role of its local buffers.
 //
-// Key and value producers and the final consumer are functors, so the first
-// pass can compute keys straight from particle coordinates and the last pass
-// can gather particle coordinates into sorted order instead of writing
-// indices.
+// Key and payload producers and the consumer are functors, so the first pass
+// computes keys and payload straight from the caller's coordinates and the
+// last pass writes the final layout.
 #pragma once
 
 #include <cuda_runtime.h>
 #include <cstdint>
 
+#include "sjcs_internal.cuh"
+
 namespace sjcs {
 
 constexpr int RS_THREADS = 512;
 constexpr int RS_ITEMS = 8;
-constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 4096 keys per tile
+constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 4096 records per tile
 constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_BITS = 8;
 constexpr int RS_BINS = 1 << RS_BITS;
 constexpr int RS_SUBHIST = 4;  // upsweep: warps share RS_SUBHIST histograms
+// dynamic shared memory of the downsweep: exchanged keys + payloads
+constexpr size_t RS_DOWN_SMEM = (size_t)RS_TILE * (sizeof(uint32_t) + sizeof(uint4));
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -36,23 +40,21 @@ __device__ __forceinline__ uint32_t lanemask_lt() {
     return m;
 }
 
+// Intermediate record arrays: keys[n] and payload[n] (uint4).
 struct KeysFromArray {
     const uint32_t* __restrict__ keys;
     __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return keys[i]; }
 };
-struct ValsFromArray {
-    const uint32_t* __restrict__ vals;
-    __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return vals[i]; }
+struct PayFromArray {
+    const uint4* __restrict__ pay;
+    __device__ __forceinline__ uint4 operator()(uint64_t i) const { return pay[i]; }
 };
-struct ValsIota {
-    __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return (uint32_t)i; }
-};
-struct SinkPairs {
+struct SinkRecords {
     uint32_t* __restrict__ keys;
-    uint32_t* __restrict__ vals;
-    __device__ __forceinline__ void operator()(uint32_t g, uint32_t k, uint32_t v) const {
+    uint4* __restrict__ pay;
+    __device__ __forceinline__ void operator()(uint32_t g, uint32_t k, const uint4& v) const {
         keys[g] = k;
-        vals[g] = v;
+        pay[g] = v;
     }
 };
 
@@ -79,15 +81,17 @@ k_radix_upsweep(KeyOp kop, uint64_t n, int shift, uint32_t* __restrict__ hist, u
     }
 }
 
-template <class KeyOp, class ValOp, class Sink>
+template <class KeyOp, class PayOp, class Sink>
 __global__ void __launch_bounds__(RS_THREADS)
-k_radix_downsweep(KeyOp kop, ValOp vop, uint64_t n, int shift,
+k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
                   const uint32_t* __restrict__ offs, uint32_t ntiles, Sink sink) {
     __shared__ uint32_t warp_cnt[RS_WARPS][RS_BINS];
     __shared__ uint32_t dstart[RS_BINS];
     __shared__ uint32_t gbase[RS_BINS];
     __shared__ uint32_t wsum[RS_BINS / 32];
-    __shared__ uint32_t xbuf[RS_TILE];
+    extern __shared__ uint4 xdyn[];
+    uint4* xpay = xdyn;                                            // [RS_TILE]
+    uint32_t* xkey = reinterpret_cast<uint32_t*>(xdyn + RS_TILE);  // [RS_TILE]
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
@@ -153,36 +157,70 @@ k_radix_downsweep(KeyOp kop, ValOp vop, uint64_t n, int shift,
         if (pos[i] != 0xffffffffu) {
             const uint32_t d = (key[i] >> shift) & (RS_BINS - 1);
             pos[i] += dstart[d] + warp_cnt[warp][d];
-            xbuf[pos[i]] = key[i];
+            const uint32_t loc = wbase + (uint32_t)i * 32u + (uint32_t)lane;
+            xkey[pos[i]] = key[i];
+            xpay[pos[i]] = pop(tile_base + loc);
         }
     }
     __syncthreads();
-
-    uint32_t okey[RS_ITEMS], og[RS_ITEMS];
 #pragma unroll
     for (int k = 0; k < RS_ITEMS; ++k) {
         const uint32_t j = (uint32_t)tid + (uint32_t)k * RS_THREADS;
         if (j < tile_n) {
-            const uint32_t kk = xbuf[j];
+            const uint32_t kk = xkey[j];
             const uint32_t d = (kk >> shift) & (RS_BINS - 1);
-            okey[k] = kk;
-            og[k] = gbase[d] + (j - dstart[d]);
+            sink(gbase[d] + (j - dstart[d]), kk, xpay[j]);
         }
     }
-    __syncthreads();
-#pragma unroll
-    for (int i = 0; i < RS_ITEMS; ++i) {
-        if (pos[i] != 0xffffffffu) {
-            const uint32_t loc = wbase + (uint32_t)i * 32u + (uint32_t)lane;
-            xbuf[pos[i]] = vop(tile_base + loc);
-        }
+}
+
+template <class KeyOp, class PayOp, class Sink>
+int radix_pass(KeyOp kop, PayOp pop, Sink sink, uint64_t n, int shift, uint32_t* hist, uint32_t ntiles,
+               cudaStream_t s) {
+    k_radix_upsweep<<<ntiles, RS_THREADS, 0, s>>>(kop, n, shift, hist, ntiles);
+    SJCS_LAUNCH_CHECK();
+    int rc = exclusive_scan_u32(hist, (uint64_t)RS_BINS * ntiles, s);
+    if (rc) return rc;
+    auto kern = k_radix_downsweep<KeyOp, PayOp, Sink>;
+    SJCS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_DOWN_SMEM));
+    kern<<<ntiles, RS_THREADS, RS_DOWN_SMEM, s>>>(kop, pop, n, shift, hist, ntiles, sink);
+    SJCS_LAUNCH_CHECK();
+    return SJCS_OK;
+}
+
+// Sort n records by their low key_bits key bits.  Pass 0 reads (kop0, pop0);
+// the last pass hands every record to `final`; passes in between ping-pong
+// through (keys_x, pay_x) and (keys_y, pay_y), arranged so that the pass
+// before the last one writes the x buffers.  hist holds RS_BINS * ntiles u32.
+template <class KeyOp0, class PayOp0, class FinalSink>
+int radix_sort_records(uint64_t n, int key_bits, KeyOp0 kop0, PayOp0 pop0, FinalSink final_sink,
+                       uint32_t* keys_x, uint4* pay_x, uint32_t* keys_y, uint4* pay_y, uint32_t* hist,
+                       cudaStream_t s) {
+    if (n == 0) return SJCS_OK;
+    const uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+    const int passes = key_bits <= 0 ? 1 : (key_bits + RS_BITS - 1) / RS_BITS;
+    for (int p = 0; p < passes; ++p) {
+        const int shift = p * RS_BITS;
+        const bool first = (p == 0), last = (p == passes - 1);
+        // record buffers written by pass p (p < passes-1): x when (passes-2-p) is even
+        const bool to_x = ((passes - 2 - p) % 2) == 0;
+        uint32_t* kout = to_x ? keys_x : keys_y;
+        uint4* vout = to_x ? pay_x : pay_y;
+        uint32_t* kin = to_x ? keys_y : keys_x;  // written by pass p-1
+        uint4* vin = to_x ? pay_y : pay_x;
+        int rc;
+        if (first && last)
+            rc = radix_pass(kop0, pop0, final_sink, n, shift, hist, ntiles, s);
+        else if (first)
+            rc = radix_pass(kop0, pop0, SinkRecords{kout, vout}, n, shift, hist, ntiles, s);
+        else if (last)
+            rc = radix_pass(KeysFromArray{keys_x}, PayFromArray{pay_x}, final_sink, n, shift, hist, ntiles, s);
+        else
+            rc = radix_pass(KeysFromArray{kin}, PayFromArray{vin}, SinkRecords{kout, vout}, n, shift, hist, ntiles,
+                            s);
+        if (rc) return rc;
     }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < RS_ITEMS; ++k) {
-        const uint32_t j = (uint32_t)tid + (uint32_t)k * RS_THREADS;
-        if (j < tile_n) sink(og[k], okey[k], xbuf[j]);
-    }
+    return SJCS_OK;
 }
 
 }  // namespace sjcs

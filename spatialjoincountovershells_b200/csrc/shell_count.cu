@@ -1,13 +1,16 @@
 // Warp-cooperative periodic multi-shell count (plain grid index).
 //
 // One warp owns one halo at a time.  For every periodic image of the halo the
-// warp turns the query box into at most a few dozen rows of cells (one row =
-// one contiguous slot range of the sorted particles), flattens the rows into
-// a single candidate sequence and lets lane l test candidates l, l+32, ...
-// so every particle load is coalesced.  Accepted candidates are binned with a
-// branch-free search of the squared-radius table in shared memory and counted
-// in per-warp shared-memory counters; the warp adds its counters to the
-// halo's row once per halo.
+// warp turns the query box into rows of cells (one row = one contiguous slot
+// range of the sorted particles), clips each row's x-extent to the sphere of
+// radius R with conservative floating-point margins (a row whose cells cannot
+// hold a particle within R is skipped), flattens the rows into one candidate
+// sequence and lets lane l test candidates l, l+32, ... so every particle load
+// is a coalesced 128-bit load.  Accepted candidates are binned through a
+// lookup table on the float bit pattern of the squared distance (one compare
+// refines the slot) and counted in per-warp shared-memory counters; the warp
+// adds its counters to the halo's row once per halo with fire-and-forget
+// reductions.
 //
 // Arithmetic follows the reference exactly (fp32, round-to-nearest, no FMA,
 // no flush-to-zero):
@@ -21,7 +24,19 @@
 //                                                       MultiRangeCount.c:31-71, Mbr.c:284-313
 // For a non-decreasing, NaN-free table "first i with dist < r2[i]" equals
 // #{i : r2[i] <= dist} and a particle is counted iff dist < r2[n-1]; other
-// tables use the literal first-match scan.
+// tables use the literal first-match scan (and no sphere clipping).
+//
+// Why the sphere clipping never drops a counted particle: a counted particle
+// has fp32 dist < r2max, and fp32 rounding of the 3 differences and 5
+// products/sums lowers the exact squared distance by at most a factor
+// (1 - 2^-24)^5, so its exact squared distance is < r2max * (1 + 1e-5) = r2p.
+// Its y lies inside its cell's y-extent, so (py - cy)^2 >= gy^2 where gy is a
+// lower bound of the halo's distance to that extent (cell edges widened by
+// 1e-3 + 2e-6*|edge|, far above the rounding of k*h and of the cell function);
+// likewise z.  Hence (px - cx)^2 < r2p - gy^2 - gz^2, and the fp32 evaluation
+// of that bound is off by at most 4 ulps of r2p < 1e-5*r2p, which is added
+// back before the square root; the x cell range then uses cx -+ (xr + 1e-3 +
+// 1e-6*(|cx| + xr)).
 #include "sjcs_internal.cuh"
 
 namespace sjcs {
@@ -32,29 +47,62 @@ constexpr int CT_THREADS = CT_WARPS * 32;
 constexpr int kMaxSmemTable = 8192;  // r2 entries held in shared memory
 constexpr int kMaxSmemRads = 1024;   // per-warp shared counters up to this many shells
 
+enum BinMode { BIN_LUT = 0, BIN_BSEARCH = 1, BIN_FIRST_MATCH = 2 };
+
 struct CountParams {
-    const float* __restrict__ xs;
-    const float* __restrict__ ys;
-    const float* __restrict__ zs;
+    const float4* __restrict__ pts;  // sorted particles (x, y, z, unused)
     const uint32_t* __restrict__ cs;
     GridGeom g;
+    float h[3];                      // cell edge per axis, 1000 / G
     const float4* __restrict__ halos;
     uint64_t nhalos;
-    const float* __restrict__ r2;  // [pad], +inf past nrads
+    const float* __restrict__ r2;    // [pad], +inf past nrads
+    const uint32_t* __restrict__ lut;
     int nrads;
     int pad;
+    int nlut;
+    uint32_t lut_k0;                 // bit pattern of r2[0]
+    int lut_shift;
     float half;
     float r2max;
+    float r2p;                       // r2max * (1 + 1e-5)
+    float r2slack;                   // r2max * 1e-5
     int periodic;
+    int prune;
     uint32_t* __restrict__ counts;
 };
 
+__device__ __forceinline__ float edge_margin(float v) { return 1e-3f + 2e-6f * fabsf(v); }
+
+// Lower bound of |c - y| over every y whose cell index is k.
+__device__ __forceinline__ float cell_gap(float c, int k, float h, int G) {
+    const float lo_e = (float)k * h, hi_e = (float)(k + 1) * h;
+    const float lo = (k == 0) ? -INFINITY : lo_e - edge_margin(lo_e);
+    const float hi = (k == G - 1) ? INFINITY : hi_e + edge_margin(hi_e);
+    return fmaxf(0.0f, fmaxf(lo - c, c - hi));
+}
+
+template <int BIN>
+__device__ __forceinline__ int bin_of(const CountParams& p, const float* __restrict__ tab,
+                                      const uint32_t* __restrict__ lut, float dist) {
+    if (BIN == BIN_LUT) {
+        const uint32_t key = __float_as_uint(dist);
+        if (key < p.lut_k0) return 0;
+        const int s = (int)lut[(key - p.lut_k0) >> p.lut_shift];
+        return s + ((tab[s] <= dist) ? 1 : 0);
+    } else {
+        int s = 0;
+        for (int step = p.pad >> 1; step > 0; step >>= 1) s += (tab[s + step - 1] <= dist) ? step : 0;
+        return s;
+    }
+}
+
 // BIG: table too large for shared memory -> table read from global memory and
 // counts added with global atomics straight into the halo's row.
-template <bool MONO, bool BIG>
+template <int BIN, bool BIG>
 __device__ __forceinline__ void count_image(const CountParams& p, float cx, float cy, float cz,
                                             uint32_t* __restrict__ sink, const float* __restrict__ tab,
-                                            int lane) {
+                                            const uint32_t* __restrict__ lut, int lane) {
     const float lox = __fsub_rn(cx, p.half), hix = __fadd_rn(cx, p.half);
     const float loy = __fsub_rn(cy, p.half), hiy = __fadd_rn(cy, p.half);
     const float loz = __fsub_rn(cz, p.half), hiz = __fadd_rn(cz, p.half);
@@ -67,18 +115,36 @@ __device__ __forceinline__ void count_image(const CountParams& p, float cx, floa
     const int y1 = (hiy != hiy) ? p.g.G[1] - 1 : cell_of(hiy, p.g.inv_h[1], p.g.G[1]);
     const int z0 = cell_of(loz, p.g.inv_h[2], p.g.G[2]);
     const int z1 = (hiz != hiz) ? p.g.G[2] - 1 : cell_of(hiz, p.g.inv_h[2], p.g.G[2]);
-    const int ny = y1 - y0 + 1;
-    const int nrows = ny * (z1 - z0 + 1);
+    const int64_t ny = y1 - y0 + 1;
+    const int64_t nrows = ny * (int64_t)(z1 - z0 + 1);
 
-    for (int rb = 0; rb < nrows; rb += 32) {
-        const int r = rb + lane;
+    for (int64_t rb = 0; rb < nrows; rb += 32) {
+        const int64_t r = rb + lane;
         uint32_t start = 0, len = 0;
         if (r < nrows) {
-            const int q = r / ny;
-            const uint64_t rowcell =
-                ((uint64_t)(z0 + q) * (uint64_t)p.g.G[1] + (uint64_t)(y0 + r - q * ny)) * (uint64_t)p.g.G[0];
-            start = __ldg(p.cs + rowcell + x0);
-            len = __ldg(p.cs + rowcell + x1 + 1) - start;
+            const int64_t q = r / ny;
+            const int yy = (int)(y0 + r - q * ny), zz = (int)(z0 + q);
+            int xa = x0, xb = x1;
+            if (p.prune) {
+                const float gy = cell_gap(cy, yy, p.h[1], p.g.G[1]);
+                const float gz = cell_gap(cz, zz, p.h[2], p.g.G[2]);
+                const float rem = __fadd_rn(__fsub_rn(__fsub_rn(p.r2p, __fmul_rn(gy, gy)), __fmul_rn(gz, gz)),
+                                            p.r2slack);
+                if (rem < 0.0f) {
+                    xb = xa - 1;  // no particle of this row can be within R
+                } else {
+                    float xr = __fsqrt_rn(rem);
+                    xr = __fadd_rn(xr, 1e-3f + 1e-6f * (fabsf(cx) + xr));
+                    const float xl = __fsub_rn(cx, xr), xh = __fadd_rn(cx, xr);
+                    xa = max(xa, cell_of(xl, p.g.inv_h[0], p.g.G[0]));
+                    if (xh == xh) xb = min(xb, cell_of(xh, p.g.inv_h[0], p.g.G[0]));
+                }
+            }
+            if (xa <= xb) {
+                const uint64_t rowcell = ((uint64_t)zz * (uint64_t)p.g.G[1] + (uint64_t)yy) * (uint64_t)p.g.G[0];
+                start = __ldg(p.cs + rowcell + xa);
+                len = __ldg(p.cs + rowcell + xb + 1) - start;
+            }
         }
         uint32_t incl = len;
 #pragma unroll
@@ -100,20 +166,14 @@ __device__ __forceinline__ void count_image(const CountParams& p, float cx, floa
             }
             const uint32_t o = __shfl_sync(0xffffffffu, off, rr);
             if (t < total) {
-                const uint32_t k = t + o;
-                const float px = __ldg(p.xs + k), py = __ldg(p.ys + k), pz = __ldg(p.zs + k);
-                const bool inb = !(px < lox) & !(hix < px) & !(py < loy) & !(hiy < py) & !(pz < loz) &
-                                 !(hiz < pz);
-                const float dx = __fsub_rn(px, cx), dy = __fsub_rn(py, cy), dz = __fsub_rn(pz, cz);
+                const float4 pp = __ldg(p.pts + (t + o));
+                const bool inb = !(pp.x < lox) & !(hix < pp.x) & !(pp.y < loy) & !(hiy < pp.y) &
+                                 !(pp.z < loz) & !(hiz < pp.z);
+                const float dx = __fsub_rn(pp.x, cx), dy = __fsub_rn(pp.y, cy), dz = __fsub_rn(pp.z, cz);
                 const float dist =
                     __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-                if (MONO) {
-                    if (inb && dist < p.r2max) {
-                        int s = 0;
-                        for (int step = p.pad >> 1; step > 0; step >>= 1)
-                            s += (tab[s + step - 1] <= dist) ? step : 0;
-                        atomicAdd(sink + s, 1u);
-                    }
+                if (BIN != BIN_FIRST_MATCH) {
+                    if (inb && dist < p.r2max) atomicAdd(sink + bin_of<BIN>(p, tab, lut, dist), 1u);
                 } else if (inb) {
                     for (int i = 0; i < p.nrads; ++i) {
                         if (dist < tab[i]) {
@@ -127,18 +187,21 @@ __device__ __forceinline__ void count_image(const CountParams& p, float cx, floa
     }
 }
 
-template <bool MONO, bool BIG>
-__global__ void __launch_bounds__(CT_THREADS) k_shell_count(CountParams p) {
+template <int BIN, bool BIG>
+__global__ void __launch_bounds__(CT_THREADS, 4) k_shell_count(CountParams p) {
     extern __shared__ uint32_t smem[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     float* r2s = reinterpret_cast<float*>(smem);
-    uint32_t* wcnt = smem + p.pad + warp * p.nrads;
+    uint32_t* luts = smem + p.pad;
+    uint32_t* wcnt = luts + p.nlut + warp * p.nrads;
     if (!BIG) {
         for (int i = tid; i < p.pad; i += CT_THREADS) r2s[i] = p.r2[i];
-        for (int i = tid; i < CT_WARPS * p.nrads; i += CT_THREADS) smem[p.pad + i] = 0u;
+        for (int i = tid; i < p.nlut; i += CT_THREADS) luts[i] = p.lut[i];
+        for (int i = tid; i < CT_WARPS * p.nrads; i += CT_THREADS) luts[p.nlut + i] = 0u;
         __syncthreads();
     }
     const float* tab = BIG ? p.r2 : r2s;
+    const uint32_t* lut = BIG ? p.lut : luts;
     const uint64_t stride = (uint64_t)gridDim.x * CT_WARPS;
     for (uint64_t h = (uint64_t)blockIdx.x * CT_WARPS + warp; h < p.nhalos; h += stride) {
         const float4 c = p.halos[h];
@@ -158,13 +221,13 @@ __global__ void __launch_bounds__(CT_THREADS) k_shell_count(CountParams p) {
             // every subset S of F, the empty set (the un-shifted search) included
             unsigned S = F;
             for (;;) {
-                count_image<MONO, BIG>(p, (S & 1u) ? sx : c.x, (S & 2u) ? sy : c.y, (S & 4u) ? sz : c.z,
-                                       sink, tab, lane);
+                count_image<BIN, BIG>(p, (S & 1u) ? sx : c.x, (S & 2u) ? sy : c.y, (S & 4u) ? sz : c.z, sink, tab,
+                                      lut, lane);
                 if (S == 0) break;
                 S = (S - 1u) & F;
             }
         } else {
-            count_image<MONO, BIG>(p, c.x, c.y, c.z, sink, tab, lane);
+            count_image<BIN, BIG>(p, c.x, c.y, c.z, sink, tab, lut, lane);
         }
         if (!BIG) {
             __syncwarp();
@@ -172,7 +235,7 @@ __global__ void __launch_bounds__(CT_THREADS) k_shell_count(CountParams p) {
                 const uint32_t v = wcnt[s];
                 if (v) {
                     wcnt[s] = 0u;
-                    row[s] += v;
+                    atomicAdd(row + s, v);  // result unused: compiles to a reduction
                 }
             }
             __syncwarp();
@@ -180,10 +243,11 @@ __global__ void __launch_bounds__(CT_THREADS) k_shell_count(CountParams p) {
     }
 }
 
-template <bool MONO, bool BIG>
+template <int BIN, bool BIG>
 int launch_variant(sjcs_ctx* ctx, const CountParams& p, size_t smem, cudaStream_t s) {
-    auto kern = k_shell_count<MONO, BIG>;
-    if (smem > 48 * 1024) SJCS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    auto kern = k_shell_count<BIN, BIG>;
+    if (smem > 48 * 1024)
+        SJCS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm = 0;
     SJCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, CT_THREADS, smem));
     if (per_sm < 1) per_sm = 1;
@@ -200,25 +264,40 @@ int launch_variant(sjcs_ctx* ctx, const CountParams& p, size_t smem, cudaStream_
 int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s) {
     if (q->nhalos == 0 || idx->n == 0) return SJCS_OK;
     CountParams p;
-    p.xs = idx->xs;
-    p.ys = idx->ys;
-    p.zs = idx->zs;
+    p.pts = idx->pts;
     p.cs = idx->cell_start;
     p.g = idx->geom;
+    for (int a = 0; a < 3; ++a) p.h[a] = 1000.0f / (float)idx->geom.G[a];
     p.halos = q->halos;
     p.nhalos = q->nhalos;
     p.r2 = q->d_r2;
+    p.lut = q->d_lut;
     p.nrads = q->nrads;
     p.pad = q->pad;
+    p.nlut = q->nlut;
+    p.lut_k0 = q->lut_k0;
+    p.lut_shift = q->lut_shift;
     p.half = q->half;
     p.r2max = q->r2max;
+    p.r2p = q->r2max * (1.0f + 1e-5f);
+    p.r2slack = q->r2max * 1e-5f;
     p.periodic = (q->flags & SJCS_QUERY_PERIODIC) ? 1 : 0;
+    p.prune = q->monotone && std::isfinite(q->r2max) ? 1 : 0;
     p.counts = q->counts;
+    const int bin = !q->monotone ? BIN_FIRST_MATCH : (q->nlut > 0 ? BIN_LUT : BIN_BSEARCH);
     const bool big = q->pad > kMaxSmemTable || q->nrads > kMaxSmemRads;
-    const size_t smem = big ? 0 : (size_t)(q->pad + CT_WARPS * q->nrads) * sizeof(uint32_t);
-    if (q->monotone)
-        return big ? launch_variant<true, true>(ctx, p, smem, s) : launch_variant<true, false>(ctx, p, smem, s);
-    return big ? launch_variant<false, true>(ctx, p, smem, s) : launch_variant<false, false>(ctx, p, smem, s);
+    if (big) p.nlut = q->nlut;  // table and LUT are read from global memory
+    const size_t smem = big ? 0 : (size_t)(q->pad + q->nlut + CT_WARPS * q->nrads) * sizeof(uint32_t);
+    switch (bin) {
+        case BIN_LUT:
+            return big ? launch_variant<BIN_LUT, true>(ctx, p, smem, s) : launch_variant<BIN_LUT, false>(ctx, p, smem, s);
+        case BIN_BSEARCH:
+            return big ? launch_variant<BIN_BSEARCH, true>(ctx, p, smem, s)
+                       : launch_variant<BIN_BSEARCH, false>(ctx, p, smem, s);
+        default:
+            return big ? launch_variant<BIN_FIRST_MATCH, true>(ctx, p, smem, s)
+                       : launch_variant<BIN_FIRST_MATCH, false>(ctx, p, smem, s);
+    }
 }
 
 }  // namespace sjcs

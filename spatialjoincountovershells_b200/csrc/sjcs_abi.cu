@@ -86,6 +86,45 @@ void host_store(uint64_t* dst, const uint64_t* src, uint64_t m, bool add) {
     for (auto& x : th) x.join();
 }
 
+// Shell lookup table over the bit patterns of squared distances (see
+// sjcs_query::d_lut).  Built only for strictly increasing, finite,
+// non-negative tables whose closest pair of values is far enough apart in bit
+// space to give at most 4096 slots; otherwise the kernel binary-searches.
+void build_shell_lut(const float* r2, int nrads, std::vector<uint32_t>* lut, uint32_t* k0_out, int* shift_out) {
+    constexpr size_t kMaxSlots = 4096;
+    lut->clear();
+    if (nrads < 2) return;
+    uint32_t prev = 0;
+    uint32_t min_gap = 0xffffffffu;
+    for (int i = 0; i < nrads; ++i) {
+        if (!std::isfinite(r2[i])) return;
+        uint32_t b;
+        std::memcpy(&b, &r2[i], 4);
+        if (b & 0x80000000u) return;  // negative or -0.0: bit order is not value order
+        if (i > 0) {
+            if (b <= prev) return;  // repeated value
+            min_gap = std::min(min_gap, b - prev);
+        }
+        prev = b;
+    }
+    uint32_t k0, kmax;
+    std::memcpy(&k0, &r2[0], 4);
+    std::memcpy(&kmax, &r2[nrads - 1], 4);
+    int shift = 0;
+    while (shift < 31 && (2u << shift) <= min_gap) ++shift;  // 2^shift <= min_gap
+    const uint64_t nslots = ((uint64_t)(kmax - 1 - k0) >> shift) + 1;
+    if (nslots > kMaxSlots) return;
+    lut->resize(nslots);
+    for (uint64_t j = 0; j < nslots; ++j) {
+        const uint32_t key = k0 + (uint32_t)(j << shift);
+        float v;
+        std::memcpy(&v, &key, 4);
+        (*lut)[j] = (uint32_t)(std::upper_bound(r2, r2 + nrads, v) - r2);  // #{r2[i] <= v}
+    }
+    *k0_out = k0;
+    *shift_out = shift;
+}
+
 int query_prepare(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride, uint64_t nhalos, const float* r2,
                   int nrads, int flags, sjcs_query* q, StreamScratch* keep) {
     (void)keep;
@@ -109,6 +148,14 @@ int query_prepare(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride, uint64_
     k_fill_f32<<<(pad + 255) / 256, 256, 0, s>>>(q->d_r2, (uint64_t)pad, INFINITY);
     SJCS_LAUNCH_CHECK();
     SJCS_CUDA_TRY(cudaMemcpyAsync(q->d_r2, r2, (size_t)nrads * sizeof(float), cudaMemcpyHostToDevice, s));
+    std::vector<uint32_t> lut;
+    if (mono) build_shell_lut(r2, nrads, &lut, &q->lut_k0, &q->lut_shift);
+    q->nlut = (int)lut.size();
+    if (!lut.empty()) {
+        SJCS_CUDA_TRY(cudaMallocAsync(&q->d_lut, lut.size() * sizeof(uint32_t), s));
+        SJCS_CUDA_TRY(cudaMemcpyAsync(q->d_lut, lut.data(), lut.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
+        // the pageable source is copied before cudaMemcpyAsync returns
+    }
     const uint64_t ncnt = nhalos * (uint64_t)nrads;
     SJCS_CUDA_TRY(cudaMallocAsync(&q->counts, (ncnt ? ncnt : 1) * sizeof(uint32_t), s));
     if (ncnt) SJCS_CUDA_TRY(cudaMemsetAsync(q->counts, 0, ncnt * sizeof(uint32_t), s));
@@ -151,6 +198,7 @@ void free_query(sjcs_query* q) {
     if (q->halos) cudaFreeAsync(q->halos, s);
     if (q->counts) cudaFreeAsync(q->counts, s);
     if (q->d_r2) cudaFreeAsync(q->d_r2, s);
+    if (q->d_lut) cudaFreeAsync(q->d_lut, s);
     cudaStreamSynchronize(s);
     if (q->h_stage) cudaFreeHost(q->h_stage);
     clear_count_events(q);
@@ -178,9 +226,7 @@ void free_index(sjcs_index* idx) {
     // Frees are ordered after the build (build stream) and after every count
     // queued on the count stream that reads this index.
     cudaStreamWaitEvent(ctx->s_count, idx->ev_ready, 0);
-    if (idx->xs) cudaFreeAsync(idx->xs, ctx->s_count);
-    if (idx->ys) cudaFreeAsync(idx->ys, ctx->s_count);
-    if (idx->zs) cudaFreeAsync(idx->zs, ctx->s_count);
+    if (idx->pts) cudaFreeAsync(idx->pts, ctx->s_count);
     if (idx->cell_start) cudaFreeAsync(idx->cell_start, ctx->s_count);
     cudaEventDestroy(idx->ev_start);
     cudaEventDestroy(idx->ev_h2d);

@@ -1,8 +1,9 @@
 // Internal declarations shared by the CUDA translation units of libsjcs.so.
 //
 // Data layout in HBM (one particle file = one index):
-//   xs[n], ys[n], zs[n]   fp32, particles sorted by cell key (SoA, so a warp
-//                         reading 32 consecutive candidates touches 3 x 128 B)
+//   pts[n]                float4 (x, y, z, unused), particles sorted by cell
+//                         key, so a warp reading 32 consecutive candidates
+//                         issues one coalesced 128-bit load per lane
 //   cell_start[ncells+1]  u32, first sorted slot of every cell; cells are
 //                         numbered x-fastest ((cz*Gy + cy)*Gx + cx), so one
 //                         (cy, cz) row of cells is one contiguous slot range.
@@ -126,9 +127,7 @@ struct sjcs_index {
     int kind;
     uint64_t n;
     sjcs::GridGeom geom;
-    float* xs;
-    float* ys;
-    float* zs;
+    float4* pts;           // n sorted particles
     uint32_t* cell_start;  // geom.ncells + 1 entries
     cudaEvent_t ev_start, ev_h2d, ev_ready;
     bool had_h2d;
@@ -148,6 +147,14 @@ struct sjcs_query {
     float4* halos;      // Morton-sorted halos, .w = original index bits
     uint32_t* counts;   // [nhalos][nrads], caller's halo order
     float* d_r2;        // [pad], entries past nrads = +inf
+    // Shell lookup on the bit pattern of dist (non-negative floats order like
+    // their bits): slot j covers keys [lut_k0 + j<<lut_shift, ...+1<<lut_shift)
+    // and holds #{i : r2[i] <= first value of the slot}; every slot holds at
+    // most one table value, so one compare against r2[slot value] finishes.
+    uint32_t* d_lut;    // [nlut]; nlut == 0: no LUT, binary search instead
+    int nlut;
+    uint32_t lut_k0;
+    int lut_shift;
     uint32_t* h_stage;  // pinned staging for count read-back
     size_t h_stage_elems;
     std::vector<cudaEvent_t> count_events;  // (start, end) pairs, one per count call since reset

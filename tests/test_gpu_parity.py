@@ -106,6 +106,8 @@ def test_radius_tables_outside_the_fast_path(ctx):
         np.array([100.0, 400.0, np.nan], np.float32),          # NaN last: R is NaN, box passes everything
         np.array([25.0], np.float32),                          # a single shell
         np.array([0.0, 0.0, 100.0, 100.0, 400.0], np.float32), # repeated edges
+        np.array([0.0, 1.0, 4.0, 9.0, 900.0], np.float32),     # zero first edge (lookup-table path)
+        np.linspace(1e-3, 900, 3000).astype(np.float32),       # too dense for the lookup table
         np.linspace(1, 3000, 2000).astype(np.float32),         # more shells than shared memory holds
     ]
     for r2 in tables:
@@ -113,6 +115,32 @@ def test_radius_tables_outside_the_fast_path(ctx):
             got = gpu_counts(ctx, [p], h, r2, periodic=periodic, hint=10.0)
             want = oracle.count(p, h, r2, periodic=periodic, brute=len(r2) < 10)
             assert np.array_equal(got, want), (r2[:4], periodic)
+
+
+@pytest.mark.parametrize("rmax", [5.0, 20.0, 0.37])
+def test_particles_on_the_search_sphere(rmax, ctx):
+    # The count kernel clips each row of cells to the sphere of radius R with
+    # conservative margins; particles on the sphere (and a few ulps either
+    # side), around halos sitting on cell edges, must all be classified exactly.
+    rng = np.random.default_rng(int(rmax * 100))
+    r2 = nat.radius_table(rmax / 50, rmax, 24)
+    R = np.float32(math.sqrt(float(r2[-1])))
+    for grid in [(1000, 400, 400), (97, 31, 13)]:
+        hx, hy, hz = 1000.0 / grid[0], 1000.0 / grid[1], 1000.0 / grid[2]
+        centres = [(500.0, 500.0, 500.0), (hx * 300, hy * 20, hz * 10), (hx * 31 + 1e-4, hy * 7, 2.5),
+                   (1000.0 - 1e-3, hy * 3, hz * 12), (0.0, 0.0, 0.0), (hx * 5, hy * 5 - 1e-4, hz * 5 + 1e-4)]
+        pts = []
+        for c in centres:
+            d = rng.normal(size=(3000, 3))
+            d /= np.linalg.norm(d, axis=1, keepdims=True)
+            for scale in (1.0, 1 - 1e-7, 1 + 1e-7, 1 - 3e-7, 1 + 3e-7):
+                pts.append((np.array(c) + d * float(R) * scale) % 1000.0)
+        p = np.concatenate(pts).astype(np.float32)
+        h = np.array(centres, np.float32)
+        got = gpu_counts(ctx, [p], h, r2, grid=grid)
+        want = oracle.count(p, h, r2, brute=True)
+        assert np.array_equal(got, want), grid
+        assert want[:, -1].sum() > 0
 
 
 def test_non_finite_and_out_of_box_coordinates(ctx):
