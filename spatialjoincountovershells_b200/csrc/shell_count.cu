@@ -42,7 +42,7 @@
 namespace sjcs {
 namespace {
 
-constexpr int CT_WARPS = 8;
+constexpr int CT_WARPS = 4;
 constexpr int CT_THREADS = CT_WARPS * 32;
 constexpr int kMaxSmemTable = 8192;  // r2 entries held in shared memory
 constexpr int kMaxSmemRads = 1024;   // per-warp shared counters up to this many shells
@@ -97,149 +97,372 @@ __device__ __forceinline__ int bin_of(const CountParams& p, const float* __restr
     }
 }
 
-// BIG: table too large for shared memory -> table read from global memory and
-// counts added with global atomics straight into the halo's row.
-template <int BIN, bool BIG>
-__device__ __forceinline__ void count_image(const CountParams& p, float cx, float cy, float cz,
-                                            uint32_t* __restrict__ sink, const float* __restrict__ tab,
-                                            const uint32_t* __restrict__ lut, int lane) {
-    const float lox = __fsub_rn(cx, p.half), hix = __fadd_rn(cx, p.half);
-    const float loy = __fsub_rn(cy, p.half), hiy = __fadd_rn(cy, p.half);
-    const float loz = __fsub_rn(cz, p.half), hiz = __fadd_rn(cz, p.half);
+// Image set-up: the query box, its cell range and the clipping constants.
+struct Image {
+    float cx, cy, cz;
+    float lox, hix, loy, hiy, loz, hiz;
+    int x0, x1, y0, y1, z0, z1;
+    int ny, nz;
+    uint32_t nrows;  // saturated at 2^31
+};
+
+__device__ __forceinline__ Image make_image(const CountParams& p, float cx, float cy, float cz) {
+    Image im;
+    im.cx = cx;
+    im.cy = cy;
+    im.cz = cz;
+    im.lox = __fsub_rn(cx, p.half);
+    im.hix = __fadd_rn(cx, p.half);
+    im.loy = __fsub_rn(cy, p.half);
+    im.hiy = __fadd_rn(cy, p.half);
+    im.loz = __fsub_rn(cz, p.half);
+    im.hiz = __fadd_rn(cz, p.half);
     // A NaN bound passes every particle on that side of the box test, so it
     // must open the cell range to the grid edge (cell_of maps NaN to cell 0,
     // which is right for a lower bound only).
-    const int x0 = cell_of(lox, p.g.inv_h[0], p.g.G[0]);
-    const int x1 = (hix != hix) ? p.g.G[0] - 1 : cell_of(hix, p.g.inv_h[0], p.g.G[0]);
-    const int y0 = cell_of(loy, p.g.inv_h[1], p.g.G[1]);
-    const int y1 = (hiy != hiy) ? p.g.G[1] - 1 : cell_of(hiy, p.g.inv_h[1], p.g.G[1]);
-    const int z0 = cell_of(loz, p.g.inv_h[2], p.g.G[2]);
-    const int z1 = (hiz != hiz) ? p.g.G[2] - 1 : cell_of(hiz, p.g.inv_h[2], p.g.G[2]);
-    const int64_t ny = y1 - y0 + 1;
-    const int64_t nrows = ny * (int64_t)(z1 - z0 + 1);
+    im.x0 = cell_of(im.lox, p.g.inv_h[0], p.g.G[0]);
+    im.x1 = (im.hix != im.hix) ? p.g.G[0] - 1 : cell_of(im.hix, p.g.inv_h[0], p.g.G[0]);
+    im.y0 = cell_of(im.loy, p.g.inv_h[1], p.g.G[1]);
+    im.y1 = (im.hiy != im.hiy) ? p.g.G[1] - 1 : cell_of(im.hiy, p.g.inv_h[1], p.g.G[1]);
+    im.z0 = cell_of(im.loz, p.g.inv_h[2], p.g.G[2]);
+    im.z1 = (im.hiz != im.hiz) ? p.g.G[2] - 1 : cell_of(im.hiz, p.g.inv_h[2], p.g.G[2]);
+    im.ny = im.y1 - im.y0 + 1;
+    im.nz = im.z1 - im.z0 + 1;
+    const uint64_t nr = (uint64_t)im.ny * (uint64_t)im.nz;
+    im.nrows = nr > 0x80000000ull ? 0x80000000u : (uint32_t)nr;
+    return im;
+}
 
-    for (int64_t rb = 0; rb < nrows; rb += 32) {
-        const int64_t r = rb + lane;
-        uint32_t start = 0, len = 0;
-        if (r < nrows) {
-            const int64_t q = r / ny;
-            const int yy = (int)(y0 + r - q * ny), zz = (int)(z0 + q);
-            int xa = x0, xb = x1;
-            if (p.prune) {
-                const float gy = cell_gap(cy, yy, p.h[1], p.g.G[1]);
-                const float gz = cell_gap(cz, zz, p.h[2], p.g.G[2]);
-                const float rem = __fadd_rn(__fsub_rn(__fsub_rn(p.r2p, __fmul_rn(gy, gy)), __fmul_rn(gz, gz)),
-                                            p.r2slack);
-                if (rem < 0.0f) {
-                    xb = xa - 1;  // no particle of this row can be within R
-                } else {
-                    float xr = __fsqrt_rn(rem);
-                    xr = __fadd_rn(xr, 1e-3f + 1e-6f * (fabsf(cx) + xr));
-                    const float xl = __fsub_rn(cx, xr), xh = __fadd_rn(cx, xr);
-                    xa = max(xa, cell_of(xl, p.g.inv_h[0], p.g.G[0]));
-                    if (xh == xh) xb = min(xb, cell_of(xh, p.g.inv_h[0], p.g.G[0]));
-                }
-            }
-            if (xa <= xb) {
-                const uint64_t rowcell = ((uint64_t)zz * (uint64_t)p.g.G[1] + (uint64_t)yy) * (uint64_t)p.g.G[0];
-                start = __ldg(p.cs + rowcell + xa);
-                len = __ldg(p.cs + rowcell + xb + 1) - start;
-            }
-        }
-        uint32_t incl = len;
-#pragma unroll
-        for (int o = 1; o < 32; o <<= 1) {
-            const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-            if (lane >= o) incl += v;
-        }
-        const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-        const uint32_t off = start - (incl - len);  // slot = t + off for t inside this row (mod 2^32)
+// Row r of the image (r < nrows) -> (y cell, z cell); exact for all r < 2^31.
+__device__ __forceinline__ void row_yz(const Image& im, uint32_t r, int* yy, int* zz) {
+    uint32_t q;
+    if (im.nrows <= (1u << 20)) {
+        // float quotient estimate: relative error < 4e-7, so for r < 2^20 it is
+        // off by at most one; corrected exactly below
+        q = (uint32_t)__fmul_rz((float)r, __frcp_rn((float)im.ny));
+        if (q * (uint32_t)im.ny > r) --q;
+        else if ((q + 1u) * (uint32_t)im.ny <= r) ++q;
+    } else {
+        q = r / (uint32_t)im.ny;
+    }
+    *yy = im.y0 + (int)(r - q * (uint32_t)im.ny);
+    *zz = im.z0 + (int)q;
+}
 
-        for (uint32_t wb = 0; wb < total; wb += 32) {
-            const uint32_t t = wb + (uint32_t)lane;
-            // row of t = #{rows j : incl_j <= t} (empty rows are skipped naturally)
-            int rr = 0;
-#pragma unroll
-            for (int b = 16; b >= 1; b >>= 1) {
-                const uint32_t v = __shfl_sync(0xffffffffu, incl, rr + b - 1);
-                rr += (v <= t) ? b : 0;
-            }
-            const uint32_t o = __shfl_sync(0xffffffffu, off, rr);
-            if (t < total) {
-                const float4 pp = __ldg(p.pts + (t + o));
-                const bool inb = !(pp.x < lox) & !(hix < pp.x) & !(pp.y < loy) & !(hiy < pp.y) &
-                                 !(pp.z < loz) & !(hiz < pp.z);
-                const float dx = __fsub_rn(pp.x, cx), dy = __fsub_rn(pp.y, cy), dz = __fsub_rn(pp.z, cz);
-                const float dist =
-                    __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
-                if (BIN != BIN_FIRST_MATCH) {
-                    if (inb && dist < p.r2max) atomicAdd(sink + bin_of<BIN>(p, tab, lut, dist), 1u);
-                } else if (inb) {
-                    for (int i = 0; i < p.nrads; ++i) {
-                        if (dist < tab[i]) {
-                            atomicAdd(sink + i, 1u);
-                            break;
-                        }
-                    }
-                }
+// Lane `lane` takes row rb + lane of the image: clip its x cells to the
+// sphere and fetch the row's first and one-past-last slots.  Returns the
+// slot range through *start / *end (empty: start == end).  gy_l / gz_l are
+// the lane-distributed gap tables of the image (valid when ny, nz <= 32).
+__device__ __forceinline__ void row_issue(const CountParams& p, const Image& im, uint32_t rb, int lane,
+                                          float gy_l, float gz_l, uint32_t* start, uint32_t* end) {
+    const uint32_t r = rb + (uint32_t)lane;
+    int yy = 0, zz = 0;
+    const bool live = r < im.nrows;
+    if (live) row_yz(im, r, &yy, &zz);
+    int xa = im.x0, xb = im.x1;
+    if (p.prune) {
+        const bool small = im.ny <= 32 && im.nz <= 32;
+        float gy = __shfl_sync(0xffffffffu, gy_l, (yy - im.y0) & 31);
+        float gz = __shfl_sync(0xffffffffu, gz_l, (zz - im.z0) & 31);
+        if (!small) {
+            gy = cell_gap(im.cy, yy, p.h[1], p.g.G[1]);
+            gz = cell_gap(im.cz, zz, p.h[2], p.g.G[2]);
+        }
+        const float rem =
+            __fadd_rn(__fsub_rn(__fsub_rn(p.r2p, __fmul_rn(gy, gy)), __fmul_rn(gz, gz)), p.r2slack);
+        if (rem < 0.0f) {
+            xb = xa - 1;  // no particle of this row can be within R
+        } else {
+            // approximate square root: its error (< 1e-6 relative) is far inside the margin
+            float xr = rem > 0.0f ? __fmul_rn(rem, rsqrtf(rem)) : 0.0f;
+            xr = __fadd_rn(xr, 1e-3f + 1e-6f * (fabsf(im.cx) + xr));
+            const float xl = __fsub_rn(im.cx, xr), xh = __fadd_rn(im.cx, xr);
+            xa = max(xa, cell_of(xl, p.g.inv_h[0], p.g.G[0]));
+            if (xh == xh) xb = min(xb, cell_of(xh, p.g.inv_h[0], p.g.G[0]));
+        }
+    }
+    uint32_t s0 = 0, s1 = 0;
+    if (live && xa <= xb) {
+        const uint64_t rowcell = ((uint64_t)zz * (uint64_t)p.g.G[1] + (uint64_t)yy) * (uint64_t)p.g.G[0];
+        s0 = __ldg(p.cs + rowcell + xa);
+        s1 = __ldg(p.cs + rowcell + xb + 1);
+    }
+    *start = s0;
+    *end = s1;
+}
+
+// Lane-distributed gap tables: lane j holds the gap of y cell y0 + j (and z).
+__device__ __forceinline__ void gap_tables(const CountParams& p, const Image& im, int lane, float* gy, float* gz) {
+    *gy = 0.0f;
+    *gz = 0.0f;
+    if (p.prune) {
+        if (lane < im.ny) *gy = cell_gap(im.cy, im.y0 + lane, p.h[1], p.g.G[1]);
+        if (lane < im.nz) *gz = cell_gap(im.cz, im.z0 + lane, p.h[2], p.g.G[2]);
+    }
+}
+
+template <int BIN, bool BIG>
+__device__ __forceinline__ void test_candidate(const CountParams& p, const Image& im, const float4 pp, bool live,
+                                               uint32_t* __restrict__ sink, const float* __restrict__ tab,
+                                               const uint32_t* __restrict__ lut) {
+    const bool inb = !(pp.x < im.lox) & !(im.hix < pp.x) & !(pp.y < im.loy) & !(im.hiy < pp.y) &
+                     !(pp.z < im.loz) & !(im.hiz < pp.z);
+    const float dx = __fsub_rn(pp.x, im.cx), dy = __fsub_rn(pp.y, im.cy), dz = __fsub_rn(pp.z, im.cz);
+    const float dist = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
+    if (BIN != BIN_FIRST_MATCH) {
+        if (live && inb && dist < p.r2max) atomicAdd(sink + bin_of<BIN>(p, tab, lut, dist), 1u);
+    } else if (live && inb) {
+        for (int i = 0; i < p.nrads; ++i) {
+            if (dist < tab[i]) {
+                atomicAdd(sink + i, 1u);
+                break;
             }
         }
     }
 }
 
+// Scan the lanes' row lengths and test every candidate of those rows,
+// two windows of 32 candidates per iteration so two loads are in flight.
 template <int BIN, bool BIG>
-__global__ void __launch_bounds__(CT_THREADS, 4) k_shell_count(CountParams p) {
+__device__ __forceinline__ void run_rows(const CountParams& p, const Image& im, uint32_t start, uint32_t end,
+                                         uint32_t* __restrict__ sink, const float* __restrict__ tab,
+                                         const uint32_t* __restrict__ lut, int lane) {
+    const uint32_t len = end - start;
+    uint32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t off = start - (incl - len);  // slot = t + off for t inside this row (mod 2^32)
+    for (uint32_t wb = 0; wb < total; wb += 64) {
+        const uint32_t t0 = wb + (uint32_t)lane, t1 = t0 + 32u;
+        // row of t = #{rows j : incl_j <= t} (empty rows are skipped naturally)
+        int r0 = 0, r1 = 0;
+#pragma unroll
+        for (int b = 16; b >= 1; b >>= 1) {
+            const uint32_t v0 = __shfl_sync(0xffffffffu, incl, r0 + b - 1);
+            const uint32_t v1 = __shfl_sync(0xffffffffu, incl, r1 + b - 1);
+            r0 += (v0 <= t0) ? b : 0;
+            r1 += (v1 <= t1) ? b : 0;
+        }
+        const uint32_t o0 = __shfl_sync(0xffffffffu, off, r0);
+        const uint32_t o1 = __shfl_sync(0xffffffffu, off, r1);
+        const bool l0 = t0 < total, l1 = t1 < total;
+        const float4 p0 = l0 ? __ldg(p.pts + (t0 + o0)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 p1 = l1 ? __ldg(p.pts + (t1 + o1)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        test_candidate<BIN, BIG>(p, im, p0, l0, sink, tab, lut);
+        test_candidate<BIN, BIG>(p, im, p1, l1, sink, tab, lut);
+    }
+}
+
+// Every row chunk of an image from chunk `first_chunk` on, synchronously.
+template <int BIN, bool BIG>
+__device__ __forceinline__ void count_image(const CountParams& p, const Image& im, uint32_t first_chunk,
+                                            uint32_t* __restrict__ sink, const float* __restrict__ tab,
+                                            const uint32_t* __restrict__ lut, int lane) {
+    float gy, gz;
+    gap_tables(p, im, lane, &gy, &gz);
+    for (uint32_t rb = first_chunk * 32u; rb < im.nrows; rb += 32u) {
+        uint32_t s0, s1;
+        row_issue(p, im, rb, lane, gy, gz, &s0, &s1);
+        run_rows<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane);
+    }
+}
+
+// Periodic images other than the un-shifted one: every non-empty subset S of
+// the flagged axes (MultiRangeCount.c:31-71).
+template <int BIN, bool BIG>
+__device__ __forceinline__ void count_shifted_images(const CountParams& p, const float4 c,
+                                                     uint32_t* __restrict__ sink, const float* __restrict__ tab,
+                                                     const uint32_t* __restrict__ lut, int lane) {
+    const float lox = __fsub_rn(c.x, p.half), hix = __fadd_rn(c.x, p.half);
+    const float loy = __fsub_rn(c.y, p.half), hiy = __fadd_rn(c.y, p.half);
+    const float loz = __fsub_rn(c.z, p.half), hiz = __fadd_rn(c.z, p.half);
+    const unsigned F = ((lox < kBoxLow) | (hix > kBoxUpp) ? 1u : 0u) |
+                       ((loy < kBoxLow) | (hiy > kBoxUpp) ? 2u : 0u) |
+                       ((loz < kBoxLow) | (hiz > kBoxUpp) ? 4u : 0u);
+    if (F == 0) return;
+    // min_oob takes precedence over max_oob on an axis (MultiRangeCount.c:38-43)
+    const float sx = (lox < kBoxLow) ? __fadd_rn(c.x, kBoxUpp) : __fsub_rn(c.x, kBoxUpp);
+    const float sy = (loy < kBoxLow) ? __fadd_rn(c.y, kBoxUpp) : __fsub_rn(c.y, kBoxUpp);
+    const float sz = (loz < kBoxLow) ? __fadd_rn(c.z, kBoxUpp) : __fsub_rn(c.z, kBoxUpp);
+    for (unsigned S = F; S != 0; S = (S - 1u) & F) {
+        const Image im = make_image(p, (S & 1u) ? sx : c.x, (S & 2u) ? sy : c.y, (S & 4u) ? sz : c.z);
+        count_image<BIN, BIG>(p, im, 0, sink, tab, lut, lane);
+    }
+}
+
+// Per-halo plan written by the planning phase (one lane per halo).
+struct HaloPlan {
+    float cx, cy, cz;
+    float lox, hix, loy, hiy, loz, hiz;
+    uint32_t row;    // the halo's row in the count array
+    uint32_t nrows;  // rows stored in the row list; kSlowPlan: count in place
+    uint32_t flags;  // periodic axes whose box crosses a face (bit a = axis a)
+};
+constexpr uint32_t kSlowPlan = 0xffffffffu;
+constexpr int kBatch = 32;    // halos per warp batch (one per lane while planning)
+constexpr int kMaxRows = 28;  // rows kept per halo (a box spans <= 5x5 rows when cells are >= R/2)
+
+// Shared memory of one warp: plans and row lists of its current batch.
+struct WarpPlans {
+    HaloPlan plan[kBatch];
+    uint32_t row_cell[kBatch][kMaxRows];  // cell-table index of the row's first cell
+    uint16_t row_len[kBatch][kMaxRows];   // number of cells of the row
+};
+
+// Planning (lane = halo): the un-shifted image's box, and every row of cells
+// the sphere can reach, clipped in x, as a cell-table index range.
+__device__ __forceinline__ void plan_halo(const CountParams& p, float4 c, bool valid, HaloPlan* pl,
+                                          uint32_t* row_cell, uint16_t* row_len) {
+    const Image im = make_image(p, c.x, c.y, c.z);
+    pl->cx = im.cx;
+    pl->cy = im.cy;
+    pl->cz = im.cz;
+    pl->lox = im.lox;
+    pl->hix = im.hix;
+    pl->loy = im.loy;
+    pl->hiy = im.hiy;
+    pl->loz = im.loz;
+    pl->hiz = im.hiz;
+    pl->row = __float_as_uint(c.w);
+    uint32_t F = 0;
+    if (p.periodic)
+        F = ((im.lox < kBoxLow) | (im.hix > kBoxUpp) ? 1u : 0u) | ((im.loy < kBoxLow) | (im.hiy > kBoxUpp) ? 2u : 0u) |
+            ((im.loz < kBoxLow) | (im.hiz > kBoxUpp) ? 4u : 0u);
+    pl->flags = F;
+    if (!valid) {
+        pl->nrows = 0;
+        return;
+    }
+    if (im.nrows > (uint32_t)kMaxRows) {
+        pl->nrows = kSlowPlan;
+        return;
+    }
+    uint32_t k = 0;
+    for (int zz = im.z0; zz <= im.z1; ++zz) {
+        const float gz = p.prune ? cell_gap(im.cz, zz, p.h[2], p.g.G[2]) : 0.0f;
+        const float rz = __fsub_rn(p.r2p, __fmul_rn(gz, gz));
+        for (int yy = im.y0; yy <= im.y1; ++yy) {
+            int xa = im.x0, xb = im.x1;
+            if (p.prune) {
+                const float gy = cell_gap(im.cy, yy, p.h[1], p.g.G[1]);
+                const float rem = __fadd_rn(__fsub_rn(rz, __fmul_rn(gy, gy)), p.r2slack);
+                if (rem < 0.0f) continue;  // no particle of this row can be within R
+                // approximate square root: its error (< 1e-6 relative) is far inside the margin
+                float xr = rem > 0.0f ? __fmul_rn(rem, rsqrtf(rem)) : 0.0f;
+                xr = __fadd_rn(xr, 1e-3f + 1e-6f * (fabsf(im.cx) + xr));
+                const float xl = __fsub_rn(im.cx, xr), xh = __fadd_rn(im.cx, xr);
+                xa = max(xa, cell_of(xl, p.g.inv_h[0], p.g.G[0]));
+                if (xh == xh) xb = min(xb, cell_of(xh, p.g.inv_h[0], p.g.G[0]));
+            }
+            if (xa > xb) continue;
+            const uint32_t rowcell = ((uint32_t)zz * (uint32_t)p.g.G[1] + (uint32_t)yy) * (uint32_t)p.g.G[0];
+            row_cell[k] = rowcell + (uint32_t)xa;
+            row_len[k] = (uint16_t)(xb - xa + 1);
+            ++k;
+        }
+    }
+    pl->nrows = k;
+}
+
+// Lane r fetches the slot range of row r of planned halo k.
+__device__ __forceinline__ void fetch_rows(const CountParams& p, const WarpPlans* wp, uint32_t k, uint32_t nrows,
+                                           int lane, uint32_t* s0, uint32_t* s1) {
+    uint32_t a = 0, b = 0;
+    if ((uint32_t)lane < nrows) {
+        const uint32_t c0 = wp->row_cell[k][lane];
+        a = __ldg(p.cs + c0);
+        b = __ldg(p.cs + c0 + wp->row_len[k][lane]);
+    }
+    *s0 = a;
+    *s1 = b;
+}
+
+// Each warp takes batches of 32 of its halos.  Planning runs one lane per
+// halo; execution runs the whole warp on one halo at a time over its planned
+// rows, while the cell-table loads of the next halo of the batch are in
+// flight.  Halos with more than 28 rows and the shifted periodic images
+// (about 3% of halos at the workload's sizes) are counted in place.
+template <int BIN, bool BIG>
+__global__ void __launch_bounds__(CT_THREADS, 8) k_shell_count(CountParams p) {
     extern __shared__ uint32_t smem[];
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    float* r2s = reinterpret_cast<float*>(smem);
-    uint32_t* luts = smem + p.pad;
+    WarpPlans* wp = reinterpret_cast<WarpPlans*>(smem) + warp;
+    float* r2s = reinterpret_cast<float*>(reinterpret_cast<WarpPlans*>(smem) + CT_WARPS);
+    uint32_t* luts = reinterpret_cast<uint32_t*>(r2s + p.pad);
     uint32_t* wcnt = luts + p.nlut + warp * p.nrads;
     if (!BIG) {
         for (int i = tid; i < p.pad; i += CT_THREADS) r2s[i] = p.r2[i];
         for (int i = tid; i < p.nlut; i += CT_THREADS) luts[i] = p.lut[i];
         for (int i = tid; i < CT_WARPS * p.nrads; i += CT_THREADS) luts[p.nlut + i] = 0u;
-        __syncthreads();
     }
+    __syncthreads();
     const float* tab = BIG ? p.r2 : r2s;
     const uint32_t* lut = BIG ? p.lut : luts;
-    const uint64_t stride = (uint64_t)gridDim.x * CT_WARPS;
-    for (uint64_t h = (uint64_t)blockIdx.x * CT_WARPS + warp; h < p.nhalos; h += stride) {
-        const float4 c = p.halos[h];
-        uint32_t* row = p.counts + (uint64_t)__float_as_uint(c.w) * (uint64_t)p.nrads;
-        uint32_t* sink = BIG ? row : wcnt;
-        if (p.periodic) {
-            const float lox = __fsub_rn(c.x, p.half), hix = __fadd_rn(c.x, p.half);
-            const float loy = __fsub_rn(c.y, p.half), hiy = __fadd_rn(c.y, p.half);
-            const float loz = __fsub_rn(c.z, p.half), hiz = __fadd_rn(c.z, p.half);
-            // min_oob takes precedence over max_oob on an axis (MultiRangeCount.c:38-43)
-            const float sx = (lox < kBoxLow) ? __fadd_rn(c.x, kBoxUpp) : __fsub_rn(c.x, kBoxUpp);
-            const float sy = (loy < kBoxLow) ? __fadd_rn(c.y, kBoxUpp) : __fsub_rn(c.y, kBoxUpp);
-            const float sz = (loz < kBoxLow) ? __fadd_rn(c.z, kBoxUpp) : __fsub_rn(c.z, kBoxUpp);
-            const unsigned F = ((lox < kBoxLow) | (hix > kBoxUpp) ? 1u : 0u) |
-                               ((loy < kBoxLow) | (hiy > kBoxUpp) ? 2u : 0u) |
-                               ((loz < kBoxLow) | (hiz > kBoxUpp) ? 4u : 0u);
-            // every subset S of F, the empty set (the un-shifted search) included
-            unsigned S = F;
-            for (;;) {
-                count_image<BIN, BIG>(p, (S & 1u) ? sx : c.x, (S & 2u) ? sy : c.y, (S & 4u) ? sz : c.z, sink, tab,
-                                      lut, lane);
-                if (S == 0) break;
-                S = (S - 1u) & F;
-            }
-        } else {
-            count_image<BIN, BIG>(p, c.x, c.y, c.z, sink, tab, lut, lane);
+    // Warp gw of W takes halos gw, gw + W, gw + 2W, ... in batches of 32, so
+    // at any moment the resident warps work on one contiguous window of the
+    // Morton order and share particle lines in L1/L2.
+    const uint64_t W = (uint64_t)gridDim.x * CT_WARPS;
+    const uint64_t gw = (uint64_t)blockIdx.x * CT_WARPS + warp;
+    const uint64_t mine = p.nhalos > gw ? (p.nhalos - gw + W - 1) / W : 0;  // halos of this warp
+
+    for (uint64_t b0 = 0; b0 < mine; b0 += kBatch) {
+        const uint32_t nb = (uint32_t)min((uint64_t)kBatch, mine - b0);
+        {
+            const bool valid = (uint32_t)lane < nb;
+            const float4 c = valid ? p.halos[(b0 + lane) * W + gw] : make_float4(0.f, 0.f, 0.f, 0.f);
+            plan_halo(p, c, valid, &wp->plan[lane], wp->row_cell[lane], wp->row_len[lane]);
         }
-        if (!BIG) {
-            __syncwarp();
-            for (int s = lane; s < p.nrads; s += 32) {
-                const uint32_t v = wcnt[s];
-                if (v) {
-                    wcnt[s] = 0u;
-                    atomicAdd(row + s, v);  // result unused: compiles to a reduction
+        __syncwarp();
+        uint32_t s0, s1;
+        {
+            const uint32_t n0 = wp->plan[0].nrows;
+            fetch_rows(p, wp, 0, n0 == kSlowPlan ? 0u : n0, lane, &s0, &s1);
+        }
+        for (uint32_t k = 0; k < nb; ++k) {
+            const HaloPlan pl = wp->plan[k];
+            // the next halo's row loads overlap this halo's tests
+            uint32_t t0 = 0, t1 = 0;
+            if (k + 1 < nb) {
+                const uint32_t nn = wp->plan[k + 1].nrows;
+                fetch_rows(p, wp, k + 1, nn == kSlowPlan ? 0u : nn, lane, &t0, &t1);
+            }
+            uint32_t* row = p.counts + (uint64_t)pl.row * (uint64_t)p.nrads;
+            uint32_t* sink = BIG ? row : wcnt;
+            Image im;
+            im.cx = pl.cx;
+            im.cy = pl.cy;
+            im.cz = pl.cz;
+            im.lox = pl.lox;
+            im.hix = pl.hix;
+            im.loy = pl.loy;
+            im.hiy = pl.hiy;
+            im.loz = pl.loz;
+            im.hiz = pl.hiz;
+            if (pl.nrows == kSlowPlan) {
+                count_image<BIN, BIG>(p, make_image(p, pl.cx, pl.cy, pl.cz), 0, sink, tab, lut, lane);
+            } else {
+                run_rows<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane);
+            }
+            if (pl.flags) count_shifted_images<BIN, BIG>(p, make_float4(pl.cx, pl.cy, pl.cz, 0.f), sink, tab, lut, lane);
+            if (!BIG) {
+                __syncwarp();
+                for (int sh = lane; sh < p.nrads; sh += 32) {
+                    const uint32_t v = wcnt[sh];
+                    if (v) {
+                        wcnt[sh] = 0u;
+                        atomicAdd(row + sh, v);  // result unused: compiles to a reduction
+                    }
                 }
+                __syncwarp();
             }
-            __syncwarp();
+            s0 = t0;
+            s1 = t1;
         }
+        __syncwarp();  // the batch's plans are read before the next batch overwrites them
     }
 }
 
@@ -287,7 +510,8 @@ int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx
     const int bin = !q->monotone ? BIN_FIRST_MATCH : (q->nlut > 0 ? BIN_LUT : BIN_BSEARCH);
     const bool big = q->pad > kMaxSmemTable || q->nrads > kMaxSmemRads;
     if (big) p.nlut = q->nlut;  // table and LUT are read from global memory
-    const size_t smem = big ? 0 : (size_t)(q->pad + q->nlut + CT_WARPS * q->nrads) * sizeof(uint32_t);
+    const size_t smem = CT_WARPS * sizeof(WarpPlans) +
+                        (big ? 0 : (size_t)(q->pad + q->nlut + CT_WARPS * q->nrads) * sizeof(uint32_t));
     switch (bin) {
         case BIN_LUT:
             return big ? launch_variant<BIN_LUT, true>(ctx, p, smem, s) : launch_variant<BIN_LUT, false>(ctx, p, smem, s);
