@@ -207,6 +207,37 @@ int sjcs_multi_range_count(sjcs_ctx *ctx, const sjcs_index *idx,
                            const float *halo_xyz, size_t stride_bytes, uint64_t nhalos,
                            const float *r2, int nrads, int flags, uint64_t *counts);
 
+/* ---- allocation-free count for small inputs ------------------------------ */
+
+/* Limits of sjcs_count_noalloc and the size of the scratch array every GPU
+ * that loads this library holds until the process exits. */
+#define SJCS_NOALLOC_MAX_PARTICLES  131072u   /* 2^17 */
+#define SJCS_NOALLOC_MAX_HALOS      32768u    /* 2^15 */
+#define SJCS_NOALLOC_MAX_CELLS      131072u   /* grid cells used for the index */
+#define SJCS_NOALLOC_MAX_SHELLS     256
+#define SJCS_NOALLOC_SCRATCH_BYTES  9734656u  /* about 9.3 MB */
+
+/* No counterpart in the reference: it exists for callers that must not have
+ * a library allocate device memory -- e.g. a host program whose framework has
+ * already reserved the GPU's memory for its own caching allocator, or a
+ * latency-critical loop that cannot absorb the synchronisation cudaMalloc
+ * and cudaFree may imply.  It builds the grid index over n particles
+ * (d_xyz, device, n*3 floats), counts the shells of nhalos halos
+ * (d_halo_xyz, device, stride as sjcs_query_create) and ADDS the counts to
+ * d_counts (device, uint32 [nhalos][nrads], caller's halo order), queued on
+ * `stream` (a cudaStream_t; NULL = default stream).  It calls no cudaMalloc,
+ * cudaFree or allocating library routine: all scratch lives in one
+ * file-scope device array of SJCS_NOALLOC_SCRATCH_BYTES.  Sizes beyond the
+ * limits above are rejected with SJCS_ERR_INVALID.  The first call on a
+ * device (that device current) looks up the array's address with
+ * cudaGetSymbolAddress; make that first call before any stream capture.
+ * All calls share the array, so calls that overlap on the GPU race: keep
+ * them on one stream.  Counts equal those of sjcs_query_count. */
+int sjcs_count_noalloc(const float *d_xyz, uint64_t n,
+                       const float *d_halo_xyz, size_t stride_bytes, uint64_t nhalos,
+                       const float *r2, int nrads, int flags,
+                       uint32_t *d_counts, void *stream);
+
 /* ---- radius schedule ----------------------------------------------------- */
 
 /* r2[i] = (float)pow(2, log2(min) + i*(log2(max)-log2(min))/(n-1)) squared in

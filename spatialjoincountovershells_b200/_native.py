@@ -80,6 +80,7 @@ _SIGS = {
     "sjcs_query_destroy": (_c.c_int, [_vp]),
     "sjcs_multi_range_count": (_c.c_int, [_vp, _vp, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _vp]),
     "sjcs_radius_table": (_c.c_int, [_c.c_double, _c.c_double, _c.c_int, _vp]),
+    "sjcs_count_noalloc": (_c.c_int, [_vp, _u64, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _vp, _vp]),
 }
 
 _HOST_SIGS = {

@@ -117,6 +117,29 @@ GridGeom auto_grid(uint64_t n, float radius_hint, const uint32_t* grid_req) {
     return g;
 }
 
+int grid_key_bits(const GridGeom& g) {
+    int key_bits = 1;
+    while (key_bits < 32 && (1ull << key_bits) < g.ncells) ++key_bits;
+    return key_bits;
+}
+
+int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, cudaStream_t s) {
+    static_assert(sizeof(Gap) == 12, "gap records are 12 bytes");
+    Gap* gaps = static_cast<Gap*>(b.gaps);
+    SJCS_CUDA_TRY(cudaMemsetAsync(b.ngaps, 0, sizeof(uint32_t), s));
+    int rc = radix_sort_records(n, grid_key_bits(g), KeysFromParticles{d_xyz, g}, PayFromParticles{d_xyz},
+                                SinkParticles{b.kfinal, reinterpret_cast<uint4*>(b.pts)}, b.kx, b.px, b.ky, b.py,
+                                b.hist, s, b.partials);
+    if (rc) return rc;
+    const uint64_t threads = n + 1;
+    const unsigned blocks = (unsigned)((threads + 255) / 256);
+    k_cell_start<<<blocks, 256, 0, s>>>(b.kfinal, n, g.ncells, b.cell_start, gaps, b.ngaps, kGridGaps);
+    SJCS_LAUNCH_CHECK();
+    k_fill_gaps<<<1024, 256, 0, s>>>(gaps, b.ngaps, kGridGaps, b.cell_start);
+    SJCS_LAUNCH_CHECK();
+    return SJCS_OK;
+}
+
 int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGeom& g,
                      sjcs_index* idx, cudaStream_t s) {
     (void)ctx;
@@ -125,41 +148,25 @@ int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGe
     SJCS_CUDA_TRY(cudaMallocAsync(&idx->pts, nalloc * sizeof(float4), s));
     SJCS_CUDA_TRY(cudaMallocAsync(&idx->cell_start, (g.ncells + 1) * sizeof(uint32_t), s));
 
-    uint32_t *kx = nullptr, *ky = nullptr, *kfinal = nullptr, *hist = nullptr;
-    uint4* px = nullptr;
-    uint4* py = nullptr;
-    Gap* gaps = nullptr;
-    uint32_t* ngaps = nullptr;
-    const uint32_t max_gaps = 1u << 16;
+    GridBuildBuffers b{};
+    b.pts = idx->pts;
+    b.cell_start = idx->cell_start;
     const uint64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
-    int key_bits = 1;
-    while (key_bits < 32 && (1ull << key_bits) < g.ncells) ++key_bits;
-    const int passes = (key_bits + RS_BITS - 1) / RS_BITS;
+    const int passes = (grid_key_bits(g) + RS_BITS - 1) / RS_BITS;
     StreamScratch scr(s);  // freed (stream-ordered) on every return path
-    SJCS_CUDA_TRY(scr.alloc(&kfinal, nalloc * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&b.kfinal, nalloc * sizeof(uint32_t)));
     if (passes > 1) {
-        SJCS_CUDA_TRY(scr.alloc(&kx, nalloc * sizeof(uint32_t)));
-        SJCS_CUDA_TRY(scr.alloc(&px, nalloc * sizeof(uint4)));
+        SJCS_CUDA_TRY(scr.alloc(&b.kx, nalloc * sizeof(uint32_t)));
+        SJCS_CUDA_TRY(scr.alloc(&b.px, nalloc * sizeof(uint4)));
     }
     if (passes > 2) {
-        SJCS_CUDA_TRY(scr.alloc(&ky, nalloc * sizeof(uint32_t)));
-        SJCS_CUDA_TRY(scr.alloc(&py, nalloc * sizeof(uint4)));
+        SJCS_CUDA_TRY(scr.alloc(&b.ky, nalloc * sizeof(uint32_t)));
+        SJCS_CUDA_TRY(scr.alloc(&b.py, nalloc * sizeof(uint4)));
     }
-    SJCS_CUDA_TRY(scr.alloc(&hist, ((uint64_t)RS_BINS * (ntiles ? ntiles : 1)) * sizeof(uint32_t)));
-    SJCS_CUDA_TRY(scr.alloc(&gaps, max_gaps * sizeof(Gap)));
-    SJCS_CUDA_TRY(scr.alloc(&ngaps, sizeof(uint32_t)));
-    SJCS_CUDA_TRY(cudaMemsetAsync(ngaps, 0, sizeof(uint32_t), s));
-
-    int rc = radix_sort_records(n, key_bits, KeysFromParticles{d_xyz, g}, PayFromParticles{d_xyz},
-                                SinkParticles{kfinal, reinterpret_cast<uint4*>(idx->pts)}, kx, px, ky, py, hist, s);
-    if (rc) return rc;
-    const uint64_t threads = n + 1;
-    const unsigned blocks = (unsigned)((threads + 255) / 256);
-    k_cell_start<<<blocks, 256, 0, s>>>(kfinal, n, g.ncells, idx->cell_start, gaps, ngaps, max_gaps);
-    SJCS_LAUNCH_CHECK();
-    k_fill_gaps<<<1024, 256, 0, s>>>(gaps, ngaps, max_gaps, idx->cell_start);
-    SJCS_LAUNCH_CHECK();
-    return SJCS_OK;
+    SJCS_CUDA_TRY(scr.alloc(&b.hist, ((uint64_t)RS_BINS * (ntiles ? ntiles : 1)) * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&b.gaps, kGridGaps * sizeof(Gap)));
+    SJCS_CUDA_TRY(scr.alloc(&b.ngaps, sizeof(uint32_t)));
+    return build_grid_into(d_xyz, n, g, b, s);
 }
 
 }  // namespace sjcs

@@ -176,10 +176,10 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
 
 template <class KeyOp, class PayOp, class Sink>
 int radix_pass(KeyOp kop, PayOp pop, Sink sink, uint64_t n, int shift, uint32_t* hist, uint32_t ntiles,
-               cudaStream_t s) {
+               cudaStream_t s, uint32_t* partials) {
     k_radix_upsweep<<<ntiles, RS_THREADS, 0, s>>>(kop, n, shift, hist, ntiles);
     SJCS_LAUNCH_CHECK();
-    int rc = exclusive_scan_u32(hist, (uint64_t)RS_BINS * ntiles, s);
+    int rc = exclusive_scan_u32(hist, (uint64_t)RS_BINS * ntiles, s, partials);
     if (rc) return rc;
     auto kern = k_radix_downsweep<KeyOp, PayOp, Sink>;
     SJCS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_DOWN_SMEM));
@@ -191,11 +191,12 @@ int radix_pass(KeyOp kop, PayOp pop, Sink sink, uint64_t n, int shift, uint32_t*
 // Sort n records by their low key_bits key bits.  Pass 0 reads (kop0, pop0);
 // the last pass hands every record to `final`; passes in between ping-pong
 // through (keys_x, pay_x) and (keys_y, pay_y), arranged so that the pass
-// before the last one writes the x buffers.  hist holds RS_BINS * ntiles u32.
+// before the last one writes the x buffers.  hist holds RS_BINS * ntiles u32;
+// partials (optional) holds the scan's scan_partials_needed(RS_BINS * ntiles).
 template <class KeyOp0, class PayOp0, class FinalSink>
 int radix_sort_records(uint64_t n, int key_bits, KeyOp0 kop0, PayOp0 pop0, FinalSink final_sink,
                        uint32_t* keys_x, uint4* pay_x, uint32_t* keys_y, uint4* pay_y, uint32_t* hist,
-                       cudaStream_t s) {
+                       cudaStream_t s, uint32_t* partials = nullptr) {
     if (n == 0) return SJCS_OK;
     const uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
     const int passes = key_bits <= 0 ? 1 : (key_bits + RS_BITS - 1) / RS_BITS;
@@ -210,14 +211,15 @@ int radix_sort_records(uint64_t n, int key_bits, KeyOp0 kop0, PayOp0 pop0, Final
         uint4* vin = to_x ? pay_y : pay_x;
         int rc;
         if (first && last)
-            rc = radix_pass(kop0, pop0, final_sink, n, shift, hist, ntiles, s);
+            rc = radix_pass(kop0, pop0, final_sink, n, shift, hist, ntiles, s, partials);
         else if (first)
-            rc = radix_pass(kop0, pop0, SinkRecords{kout, vout}, n, shift, hist, ntiles, s);
+            rc = radix_pass(kop0, pop0, SinkRecords{kout, vout}, n, shift, hist, ntiles, s, partials);
         else if (last)
-            rc = radix_pass(KeysFromArray{keys_x}, PayFromArray{pay_x}, final_sink, n, shift, hist, ntiles, s);
+            rc = radix_pass(KeysFromArray{keys_x}, PayFromArray{pay_x}, final_sink, n, shift, hist, ntiles, s,
+                            partials);
         else
             rc = radix_pass(KeysFromArray{kin}, PayFromArray{vin}, SinkRecords{kout, vout}, n, shift, hist, ntiles,
-                            s);
+                            s, partials);
         if (rc) return rc;
     }
     return SJCS_OK;

@@ -87,13 +87,14 @@ __global__ void __launch_bounds__(SC_THREADS) k_scan_apply(uint32_t* __restrict_
 
 }  // namespace
 
-int exclusive_scan_u32(uint32_t* d_data, uint64_t m, cudaStream_t s) {
+uint64_t scan_partials_needed(uint64_t m) { return (m + SC_CHUNK - 1) / SC_CHUNK; }
+
+int exclusive_scan_u32(uint32_t* d_data, uint64_t m, cudaStream_t s, uint32_t* partials) {
     if (m == 0) return SJCS_OK;
     const uint64_t nb = (m + SC_CHUNK - 1) / SC_CHUNK;
     if (nb > 0xffffffffull) return fail(SJCS_ERR_INVALID, "scan too large (%llu)", (unsigned long long)m);
-    uint32_t* partials = nullptr;
     StreamScratch scr(s);
-    SJCS_CUDA_TRY(scr.alloc(&partials, nb * sizeof(uint32_t)));
+    if (!partials) SJCS_CUDA_TRY(scr.alloc(&partials, nb * sizeof(uint32_t)));
     k_scan_reduce<<<(unsigned)nb, SC_THREADS, 0, s>>>(d_data, m, partials);
     SJCS_LAUNCH_CHECK();
     k_scan_partials<<<1, SC_THREADS, 0, s>>>(partials, (uint32_t)nb);

@@ -181,6 +181,26 @@ int sort_halos(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride_bytes, uint
 int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx,
                        cudaStream_t s);
 
-// scan.cu: exclusive prefix sum of m u32 values, in place.
-int exclusive_scan_u32(uint32_t* d_data, uint64_t m, cudaStream_t s);
+// scan.cu: exclusive prefix sum of m u32 values, in place.  `partials`
+// (scan_partials_needed(m) u32) may be given; otherwise it is allocated.
+int exclusive_scan_u32(uint32_t* d_data, uint64_t m, cudaStream_t s, uint32_t* partials = nullptr);
+uint64_t scan_partials_needed(uint64_t m);
+
+// index_build.cu: the grid build on caller-provided buffers (no allocation).
+struct GridBuildBuffers {
+    float4* pts;          // n sorted particles (output)
+    uint32_t* cell_start; // ncells + 1 (output)
+    uint32_t* kfinal;     // n
+    uint32_t* kx;         // n (needed when the key has more than 8 bits)
+    uint4* px;            // n
+    uint32_t* ky;         // n (needed when the key has more than 16 bits)
+    uint4* py;            // n
+    uint32_t* hist;       // 256 * ceil(n / 4096)
+    uint32_t* partials;   // scan_partials_needed(256 * ceil(n / 4096))
+    void* gaps;           // kGridGaps gap records (12 bytes each)
+    uint32_t* ngaps;      // 1
+};
+constexpr uint32_t kGridGaps = 1u << 16;
+int grid_key_bits(const GridGeom& g);
+int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, cudaStream_t s);
 }  // namespace sjcs
