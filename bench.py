@@ -254,13 +254,22 @@ def run_ours(args, w, dist, rank, world, local):
     pnp = parts_h.numpy()
     from spatialjoincountovershells_b200._native import _hcheck, host_lib
     _hcheck(host_lib().sjcs_gen_uniform_particles(w["pseed"], nf, n, pnp.ctypes.data))
+    all_halos = nat.gen_uniform_halos(w["hseed"], nh)
+    if args.halo_slab is not None:
+        all_halos = all_halos[all_halos["point"][:, 2] < args.halo_slab]
+        nh = w["nhalos"] = len(all_halos)
     halos_pinned = torch.empty((nh * 24,), dtype=torch.uint8, pin_memory=True)
     halos_np = halos_pinned.numpy().view(nat.HALO_DTYPE)
-    halos_np[:] = nat.gen_uniform_halos(w["hseed"], nh)
+    halos_np[:] = all_halos
+    del all_halos
     out_h = torch.empty((nh * nr,), dtype=torch.int64, pin_memory=True)
     out_np = out_h.numpy().view(np.uint64).reshape(nh, nr)
 
     ctx = nat.Context(local)
+    # grow the device pool once, so no step takes new memory from the driver:
+    # K+1 queries, 4 indexes and one build's scratch
+    idx_bytes = n * 16 + int(1.6 * n + 4096) * 4
+    ctx.reserve((args.steps + 1) * nh * (16 + 4 * nr + 48) + 4 * idx_bytes + n * 44 + (1 << 30))
     s_build = torch.cuda.ExternalStream(ctx.stream(0))
     s_count = torch.cuda.ExternalStream(ctx.stream(1))
 
@@ -470,6 +479,8 @@ def main():
     ap.add_argument("--files", type=int, default=None, help="override the number of particle files")
     ap.add_argument("--halos", type=int, default=None, help="override the number of halos (same density)")
     ap.add_argument("--no-e2e", action="store_true", help="skip the host-buffer leg (profiling runs)")
+    ap.add_argument("--halo-slab", type=float, default=None,
+                    help="keep only halos with z < SLAB (profiling at full halo density on fewer halos)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     args = ap.parse_args()

@@ -107,6 +107,15 @@ int sjcs_ctx_destroy(sjcs_ctx *ctx);
 int sjcs_ctx_sync(sjcs_ctx *ctx);
 /* Number of streaming multiprocessors of the context's device. */
 int sjcs_ctx_num_sms(const sjcs_ctx *ctx, int *out);
+/* Device memory is taken from the device's stream-ordered pool, which keeps
+ * freed blocks for reuse.  sjcs_ctx_reserve grows the pool to hold at least
+ * `bytes` (so later builds and queries of that size take no new memory from
+ * the driver); sjcs_ctx_trim returns every unused block to the driver.  Both
+ * wait for the context's work.  *free_bytes / *pool_bytes report the device's
+ * free memory and the pool's size (either may be NULL). */
+int sjcs_ctx_reserve(sjcs_ctx *ctx, uint64_t bytes);
+int sjcs_ctx_trim(sjcs_ctx *ctx);
+int sjcs_ctx_memory(sjcs_ctx *ctx, uint64_t *free_bytes, uint64_t *pool_bytes);
 /* The context's CUDA streams (cudaStream_t): which = 0 build stream (copies and
  * index builds), 1 count stream (halo preparation, counts, read-back).  Lets a
  * caller order its own work or timing events against the library's. */

@@ -59,6 +59,9 @@ _SIGS = {
     "sjcs_ctx_sync": (_c.c_int, [_vp]),
     "sjcs_ctx_num_sms": (_c.c_int, [_vp, _c.POINTER(_c.c_int)]),
     "sjcs_ctx_stream": (_c.c_int, [_vp, _c.c_int, _pp]),
+    "sjcs_ctx_reserve": (_c.c_int, [_vp, _u64]),
+    "sjcs_ctx_trim": (_c.c_int, [_vp]),
+    "sjcs_ctx_memory": (_c.c_int, [_vp, _c.POINTER(_u64), _c.POINTER(_u64)]),
     "sjcs_launch_counter": (_c.c_uint64, []),
     "sjcs_host_alloc": (_c.c_int, [_c.c_size_t, _pp]),
     "sjcs_host_free": (_c.c_int, [_vp]),
@@ -193,6 +196,19 @@ class Context:
 
     def sync(self) -> None:
         _check(lib().sjcs_ctx_sync(self._h))
+
+    def reserve(self, nbytes: int) -> None:
+        """Grow the device memory pool to hold at least nbytes (no new driver allocations later)."""
+        _check(lib().sjcs_ctx_reserve(self._h, int(nbytes)))
+
+    def trim(self) -> None:
+        """Return the pool's unused memory to the driver."""
+        _check(lib().sjcs_ctx_trim(self._h))
+
+    def memory(self) -> dict:
+        f, p = _u64(), _u64()
+        _check(lib().sjcs_ctx_memory(self._h, _c.byref(f), _c.byref(p)))
+        return {"free_bytes": f.value, "pool_bytes": p.value}
 
     def stream(self, which: int) -> int:
         """cudaStream_t of the build (0) or count (1) stream, as an integer."""

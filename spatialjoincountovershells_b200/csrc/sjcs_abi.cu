@@ -364,6 +364,57 @@ int sjcs_ctx_stream(const sjcs_ctx* ctx, int which, void** stream) {
 
 uint64_t sjcs_launch_counter(void) { return g_launches.load(); }
 
+int sjcs_ctx_reserve(sjcs_ctx* ctx, uint64_t bytes) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_build));
+    SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_count));
+    if (bytes == 0) return SJCS_OK;
+    void* p = nullptr;
+    cudaError_t e = cudaMallocAsync(&p, bytes, ctx->s_count);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return fail(SJCS_ERR_NOMEM, "cannot reserve %llu bytes: %s", (unsigned long long)bytes, cudaGetErrorString(e));
+    }
+    SJCS_CUDA_TRY(cudaFreeAsync(p, ctx->s_count));
+    SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_count));
+    return SJCS_OK;
+}
+
+int sjcs_ctx_trim(sjcs_ctx* ctx) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_build));
+    SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_count));
+    cudaMemPool_t pool;
+    SJCS_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+    SJCS_CUDA_TRY(cudaMemPoolTrimTo(pool, 0));
+    return SJCS_OK;
+}
+
+int sjcs_ctx_memory(sjcs_ctx* ctx, uint64_t* free_bytes, uint64_t* pool_bytes) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    if (free_bytes) {
+        size_t f = 0, t = 0;
+        SJCS_CUDA_TRY(cudaMemGetInfo(&f, &t));
+        *free_bytes = f;
+    }
+    if (pool_bytes) {
+        cudaMemPool_t pool;
+        SJCS_CUDA_TRY(cudaDeviceGetDefaultMemPool(&pool, ctx->device));
+        uint64_t v = 0;
+        SJCS_CUDA_TRY(cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &v));
+        *pool_bytes = v;
+    }
+    return SJCS_OK;
+}
+
 int sjcs_ctx_num_sms(const sjcs_ctx* ctx, int* out) {
     if (!valid_ctx(ctx) || !out) return fail(SJCS_ERR_INVALID, "invalid argument");
     *out = ctx->num_sms;
