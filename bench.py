@@ -311,6 +311,9 @@ def run_ours(args, w, dist, rank, world, local):
             qs = []
             for _ in range(K):
                 q = step()
+                # a step is one job: the next one starts when this one is done,
+                # so builds never run ahead into the next step's files
+                q.wait()
                 if keep_queries:
                     qs.append(q)
                 else:
