@@ -125,17 +125,22 @@ int grid_key_bits(const GridGeom& g) {
 
 int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, cudaStream_t s) {
     static_assert(sizeof(Gap) == 12, "gap records are 12 bytes");
-    Gap* gaps = static_cast<Gap*>(b.gaps);
-    SJCS_CUDA_TRY(cudaMemsetAsync(b.ngaps, 0, sizeof(uint32_t), s));
     int rc = radix_sort_records(n, grid_key_bits(g), KeysFromParticles{d_xyz, g}, PayFromParticles{d_xyz},
                                 SinkParticles{b.kfinal, reinterpret_cast<uint4*>(b.pts)}, b.kx, b.px, b.ky, b.py,
                                 b.hist, s, b.partials);
     if (rc) return rc;
+    return fill_cell_table(b.kfinal, n, g.ncells, b.cell_start, b.gaps, b.ngaps, s);
+}
+
+int fill_cell_table(const uint32_t* sorted_cells, uint64_t n, uint64_t ncells, uint32_t* cell_start, void* gaps,
+                    uint32_t* ngaps, cudaStream_t s) {
+    SJCS_CUDA_TRY(cudaMemsetAsync(ngaps, 0, sizeof(uint32_t), s));
     const uint64_t threads = n + 1;
     const unsigned blocks = (unsigned)((threads + 255) / 256);
-    k_cell_start<<<blocks, 256, 0, s>>>(b.kfinal, n, g.ncells, b.cell_start, gaps, b.ngaps, kGridGaps);
+    k_cell_start<<<blocks, 256, 0, s>>>(sorted_cells, n, ncells, cell_start, static_cast<Gap*>(gaps), ngaps,
+                                        kGridGaps);
     SJCS_LAUNCH_CHECK();
-    k_fill_gaps<<<1024, 256, 0, s>>>(gaps, b.ngaps, kGridGaps, b.cell_start);
+    k_fill_gaps<<<1024, 256, 0, s>>>(static_cast<Gap*>(gaps), ngaps, kGridGaps, cell_start);
     SJCS_LAUNCH_CHECK();
     return SJCS_OK;
 }

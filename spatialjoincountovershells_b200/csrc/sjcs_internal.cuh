@@ -203,4 +203,7 @@ struct GridBuildBuffers {
 constexpr uint32_t kGridGaps = 1u << 16;
 int grid_key_bits(const GridGeom& g);
 int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, cudaStream_t s);
+// cell_start[c] = first slot of cell c, from the cell ids of the sorted particles.
+int fill_cell_table(const uint32_t* sorted_cells, uint64_t n, uint64_t ncells, uint32_t* cell_start, void* gaps,
+                    uint32_t* ngaps, cudaStream_t s);
 }  // namespace sjcs
