@@ -53,7 +53,16 @@ extern "C" {
 
 /* index kinds */
 #define SJCS_INDEX_GRID     0 /* uniform cell grid: particles radix-sorted by cell, cell-offset table */
-#define SJCS_INDEX_LEARNED  1 /* Morton-sorted particles + two-level piecewise-linear rank model */
+#define SJCS_INDEX_LEARNED  1 /* particles sorted by 63-bit Morton key; cell ranks from a two-level
+                                 piecewise-linear model (1 root + 4096 fp32 linear leaves, per-leaf
+                                 max error) corrected by a bounded exact search; the Morton
+                                 cell-offset table is kept as fallback and judge */
+#define SJCS_INDEX_MORTON   2 /* particles sorted by 63-bit Morton key, plain Morton cell-offset table */
+
+/* index option flags */
+#define SJCS_INDEX_VERIFY   0x1 /* learned kind: after training, compare the corrected model rank of
+                                   every cell boundary with the offset table; on any mismatch the
+                                   index answers from the table */
 
 /* query flags */
 #define SJCS_QUERY_PERIODIC     0x1 /* periodic images, as multiRangeCountWithPriodicBoundArraySTR */
@@ -66,11 +75,27 @@ typedef struct sjcs_query sjcs_query; /* device-resident halos + radius table + 
 /* Build options.  Zero-initialised options select an automatic grid for the
  * plain index (sized from n and radius_hint). */
 typedef struct sjcs_index_opts {
-    int      kind;         /* SJCS_INDEX_GRID or SJCS_INDEX_LEARNED */
+    int      kind;         /* SJCS_INDEX_GRID, SJCS_INDEX_LEARNED or SJCS_INDEX_MORTON */
     float    radius_hint;  /* largest search radius expected (sqrt of r2[nrads-1]); 0 = unknown */
-    uint32_t grid[3];      /* cells per axis (x, y, z) for SJCS_INDEX_GRID; 0 = automatic */
-    uint32_t reserved[4];  /* must be zero */
+    uint32_t grid[3];      /* grid kind: cells per axis (x, y, z), 0 = automatic.  Morton kinds:
+                              grid[0] = cell level L in [1,10] (cells of 1000/2^L per axis,
+                              8^L + 1 table entries), 0 = automatic; grid[1], grid[2] zero */
+    uint32_t flags;        /* SJCS_INDEX_VERIFY */
+    uint32_t reserved[3];  /* must be zero */
 } sjcs_index_opts;
+
+/* Training record of a learned index (after sjcs_index_wait). */
+typedef struct sjcs_learned_info {
+    uint32_t level;       /* Morton cell level of the lookups */
+    uint32_t leaves;      /* leaf models (4096) */
+    uint32_t nonempty;    /* leaves holding at least one key */
+    uint32_t max_err;     /* largest per-leaf error bound, in ranks */
+    double   mean_err;    /* mean error bound over non-empty leaves */
+    uint64_t checked;     /* cell boundaries judged against the table (0 without SJCS_INDEX_VERIFY) */
+    uint64_t mismatches;  /* judged lookups that disagreed (> 0: the index answers from the table) */
+    float    sort_ms;     /* key, radix sort and offset table kernels */
+    float    train_ms;    /* training (and judge) kernels */
+} sjcs_learned_info;
 
 /* Timing from CUDA events on the stream that ran the work (milliseconds; 0
  * where not applicable).  For an index: its copy and build.  For a query: the
@@ -152,9 +177,12 @@ int sjcs_index_build_device(sjcs_ctx *ctx, const float *d_xyz, uint64_t n,
 int sjcs_index_wait(sjcs_index *idx);
 /* Number of particles in the index (getNumberOfDataArraySTR, ArraySTR.h:58). */
 int sjcs_index_size(const sjcs_index *idx, uint64_t *out);
-/* Cells per axis actually used by a grid index (or the Morton leaf grid of a
- * learned index). */
+/* Cells per axis actually used by a grid index (2^L per axis for the Morton
+ * kinds). */
 int sjcs_index_grid(const sjcs_index *idx, uint32_t out[3]);
+/* Training record of a learned index; waits for the build.  No counterpart in
+ * the reference (its R-tree has no learned component). */
+int sjcs_index_learned_info(sjcs_index *idx, sjcs_learned_info *out);
 /* Timing of the build (valid after sjcs_index_wait). */
 int sjcs_index_timing(const sjcs_index *idx, sjcs_timing *out);
 /* Release the index after all queued work that reads it

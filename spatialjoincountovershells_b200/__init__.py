@@ -20,6 +20,8 @@ from ._native import (  # noqa: F401
     HALO_DTYPE,
     INDEX_GRID,
     INDEX_LEARNED,
+    INDEX_MORTON,
+    INDEX_VERIFY,
     QUERY_NONPERIODIC,
     QUERY_PERIODIC,
     Context,

@@ -14,6 +14,8 @@ host_lib_path = _PKG / "lib" / "libsjcs_host.so"
 
 INDEX_GRID = 0
 INDEX_LEARNED = 1
+INDEX_MORTON = 2
+INDEX_VERIFY = 0x1
 QUERY_NONPERIODIC = 0
 QUERY_PERIODIC = 1
 
@@ -38,7 +40,13 @@ class SjcsError(RuntimeError):
 
 class sjcs_index_opts(_c.Structure):
     _fields_ = [("kind", _c.c_int), ("radius_hint", _c.c_float), ("grid", _c.c_uint32 * 3),
-                ("reserved", _c.c_uint32 * 4)]
+                ("flags", _c.c_uint32), ("reserved", _c.c_uint32 * 3)]
+
+
+class sjcs_learned_info(_c.Structure):
+    _fields_ = [("level", _c.c_uint32), ("leaves", _c.c_uint32), ("nonempty", _c.c_uint32),
+                ("max_err", _c.c_uint32), ("mean_err", _c.c_double), ("checked", _c.c_uint64),
+                ("mismatches", _c.c_uint64), ("sort_ms", _c.c_float), ("train_ms", _c.c_float)]
 
 
 class sjcs_timing(_c.Structure):
@@ -70,6 +78,7 @@ _SIGS = {
     "sjcs_index_wait": (_c.c_int, [_vp]),
     "sjcs_index_size": (_c.c_int, [_vp, _c.POINTER(_u64)]),
     "sjcs_index_grid": (_c.c_int, [_vp, _c.POINTER(_c.c_uint32)]),
+    "sjcs_index_learned_info": (_c.c_int, [_vp, _c.POINTER(sjcs_learned_info)]),
     "sjcs_index_timing": (_c.c_int, [_vp, _c.POINTER(sjcs_timing)]),
     "sjcs_index_destroy": (_c.c_int, [_vp]),
     "sjcs_query_create": (_c.c_int, [_vp, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _pp]),
@@ -227,14 +236,20 @@ class Context:
     def __exit__(self, *exc):
         self.close()
 
-    def build_index(self, xyz, radius_hint: float = 0.0, grid=None, kind: int = INDEX_GRID) -> "Index":
-        """Index over particles: host array (n,3) float32, or a CUDA tensor (device path)."""
+    def build_index(self, xyz, radius_hint: float = 0.0, grid=None, kind: int = INDEX_GRID,
+                    level: int = 0, verify: bool = False) -> "Index":
+        """Index over particles: host array (n,3) float32, or a CUDA tensor (device path).
+        kind: INDEX_GRID (grid = cells per axis), INDEX_MORTON or INDEX_LEARNED (level =
+        Morton cell level, 0 = automatic; verify = judge the model against the table)."""
         opts = sjcs_index_opts()
         opts.kind = kind
         opts.radius_hint = float(radius_hint)
         if grid is not None:
             for a in range(3):
                 opts.grid[a] = int(grid[a])
+        if kind != INDEX_GRID:
+            opts.grid[0] = int(level)
+        opts.flags = INDEX_VERIFY if verify else 0
         h = _vp()
         if _is_cuda(xyz):
             n = xyz.numel() // 3
@@ -303,6 +318,12 @@ class Index:
         t = sjcs_timing()
         _check(lib().sjcs_index_timing(self._h, _c.byref(t)))
         return {"h2d_ms": t.h2d_ms, "build_ms": t.build_ms}
+
+    def learned_info(self) -> dict:
+        """Training record of a learned index (waits for the build)."""
+        li = sjcs_learned_info()
+        _check(lib().sjcs_index_learned_info(self._h, _c.byref(li)))
+        return {f: getattr(li, f) for f, _ in sjcs_learned_info._fields_}
 
     def destroy(self) -> None:
         if self._h:

@@ -23,7 +23,10 @@ LIB = PKG / "lib"
 BIN = PKG / "bin"
 INCLUDE = ROOT / "include"
 
-CUDA_SOURCES = ["sjcs_abi.cu", "index_build.cu", "query_prep.cu", "shell_count.cu", "scan.cu", "noalloc.cu"]
+CUDA_SOURCES = [
+    "sjcs_abi.cu", "index_build.cu", "learned_index.cu", "query_prep.cu", "shell_count.cu", "morton_count.cu",
+    "scan.cu", "noalloc.cu",
+]
 HOST_SOURCES = ["sjcs_io.c", "sjcs_gen.c"]
 
 # Exact fp32 semantics: no fast-math, no FMA contraction anywhere (the

@@ -1,0 +1,115 @@
+// Morton-ordered index: key layout, the two-level piecewise-linear rank model
+// and its exact corrected lookup.  Shared by the build (learned_index.cu) and
+// the count kernel (morton_count.cu).
+//
+// Key: 21 bits per axis, q = clamp(floor(v * 2^21/1000), 0, 2^21 - 1) (the
+// same monotone cell function as the grid, so NaN -> 0 and out-of-box values
+// clamp into the edge cells), interleaved x-lowest into a 63-bit code.  The
+// level-L cell of a particle is the key's top 3L bits (L <= 21); cells of one
+// level are contiguous key ranges, so a level-L cell is the slot range
+// [lower_bound(c << (63-3L)), lower_bound((c+1) << (63-3L))).
+//
+// HBM layout of a Morton index over n particles:
+//   pts[n]              float4 (x, y, z, level-10 prefix bits), sorted by key
+//   table[8^L + 1]      u32 plain offset table of the index's cell level L
+//   leaves[4096]        LearnedLeaf, root (one LearnedRoot)   (learned kind)
+//
+// Rank model (learned kind): the root maps a key to leaf
+// j = (key - kmin) >> shift, the smallest shift that puts kmax in leaf 4095
+// (a linear root with slope 2^-shift, exact in integers).  Leaf j holds the
+// exact first rank r0 of its key range, the first key `anchor` and an fp32
+// slope; its prediction P(q) = r0 + min(trunc(fp32((q - anchor)) * slope), r1 - r0)
+// (P(q) = r0 for q <= anchor) is monotone in q.  Training records
+// err = max over the leaf's keys k_i of |P(k_i) - i|.  For a query key q in
+// leaf j the true lower bound t satisfies
+//     t < r1  =>  P(q) <= P(k_t) <= t + err
+//     t > r0  =>  t - 1 - err <= P(k_{t-1}) <= P(q)
+// so t lies in [max(r0, P - err), min(r1, P + err + 1)], and a binary search
+// over that window (the bounded exact correction) returns t exactly.
+#pragma once
+
+#include "sjcs_internal.cuh"
+
+namespace sjcs {
+
+constexpr int kMortonBits = 21;
+constexpr float kMortonScale = 2097.152f;  // 2^21 / 1000
+constexpr int kLeafBits = 12;
+constexpr uint32_t kLeaves = 1u << kLeafBits;  // 4096 leaves
+constexpr int kPrefixLevel = 10;               // pts[i].w holds the key's top 30 bits
+constexpr int kMaxMortonLevel = 10;
+
+struct LearnedLeaf {
+    unsigned long long anchor;  // first key of the leaf (0 if empty)
+    uint32_t r0, r1;            // exact rank range of the leaf's keys
+    float slope;                // ranks per key unit
+    uint32_t err;               // max |P(k_i) - i| over the leaf's keys
+};
+static_assert(sizeof(LearnedLeaf) == 24, "leaf records are 24 bytes");
+
+struct LearnedRoot {
+    unsigned long long kmin, kmax;
+    uint32_t shift;
+    uint32_t n;
+    unsigned long long checked;     // cell boundaries compared with the table
+    unsigned long long mismatches;  // lookups that disagreed (then the table is used)
+    unsigned long long sum_err;     // sum of the leaves' err (non-empty leaves)
+    uint32_t max_err;
+    uint32_t nonempty;
+};
+
+__device__ __forceinline__ uint64_t spread3_21(uint32_t v) {
+    uint64_t x = v & 0x1fffffu;
+    x = (x | (x << 32)) & 0x001f00000000ffffull;
+    x = (x | (x << 16)) & 0x001f0000ff0000ffull;
+    x = (x | (x << 8)) & 0x100f00f00f00f00full;
+    x = (x | (x << 4)) & 0x10c30c30c30c30c3ull;
+    x = (x | (x << 2)) & 0x1249249249249249ull;
+    return x;
+}
+
+__device__ __forceinline__ uint32_t morton_q(float v) { return (uint32_t)cell_of(v, kMortonScale, 1 << kMortonBits); }
+
+__device__ __forceinline__ uint64_t morton63(float x, float y, float z) {
+    return spread3_21(morton_q(x)) | (spread3_21(morton_q(y)) << 1) | (spread3_21(morton_q(z)) << 2);
+}
+
+// Code of cell (x, y, z) at a level <= 10 (30 bits).
+__device__ __forceinline__ uint32_t morton_cell(uint32_t x, uint32_t y, uint32_t z) {
+    return spread3_10(x) | (spread3_10(y) << 1) | (spread3_10(z) << 2);
+}
+
+__device__ __forceinline__ uint32_t leaf_of(const LearnedRoot& rt, uint64_t key) {
+    return (uint32_t)((key - rt.kmin) >> rt.shift);
+}
+
+__device__ __forceinline__ uint32_t leaf_predict(const LearnedLeaf& lf, uint64_t q) {
+    if (q <= lf.anchor) return lf.r0;
+    const float off = fminf(__fmul_rn(__ull2float_rn(q - lf.anchor), lf.slope), 4.0e9f);
+    const uint32_t d = (uint32_t)off;  // off >= 0: truncation is floor
+    const uint32_t span = lf.r1 - lf.r0;
+    return lf.r0 + (d < span ? d : span);
+}
+
+// Exact lower bound of q (a cell boundary: q's low 33 bits are zero) among
+// the sorted keys, from the model and a bounded binary search over the
+// level-10 prefixes in pts[].w.
+__device__ __forceinline__ uint32_t learned_rank(const LearnedRoot& rt, const LearnedLeaf* __restrict__ leaves,
+                                                 const uint32_t* __restrict__ wpref, uint64_t q) {
+    if (q <= rt.kmin) return 0u;
+    if (q > rt.kmax) return rt.n;
+    const LearnedLeaf lf = leaves[leaf_of(rt, q)];
+    const uint32_t P = leaf_predict(lf, q);
+    uint32_t lo = (P - lf.r0 > lf.err) ? P - lf.err : lf.r0;
+    const uint64_t hi64 = (uint64_t)P + lf.err + 1ull;
+    uint32_t hi = hi64 < (uint64_t)lf.r1 ? (uint32_t)hi64 : lf.r1;
+    const uint32_t qp = (uint32_t)(q >> 33);
+    while (lo < hi) {
+        const uint32_t mid = lo + ((hi - lo) >> 1);
+        if (__ldg(wpref + 4ull * mid) < qp) lo = mid + 1u;
+        else hi = mid;
+    }
+    return lo;
+}
+
+}  // namespace sjcs

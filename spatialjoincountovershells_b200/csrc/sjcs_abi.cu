@@ -7,6 +7,7 @@
 #include <new>
 #include <thread>
 
+#include "morton.cuh"
 #include "sjcs_internal.cuh"
 
 namespace sjcs {
@@ -217,6 +218,7 @@ sjcs_index* new_index(sjcs_ctx* ctx) {
     cudaEventCreate(&idx->ev_start);
     cudaEventCreate(&idx->ev_h2d);
     cudaEventCreate(&idx->ev_ready);
+    cudaEventCreate(&idx->ev_train0);
     return idx;
 }
 
@@ -228,6 +230,9 @@ void free_index(sjcs_index* idx) {
     cudaStreamWaitEvent(ctx->s_count, idx->ev_ready, 0);
     if (idx->pts) cudaFreeAsync(idx->pts, ctx->s_count);
     if (idx->cell_start) cudaFreeAsync(idx->cell_start, ctx->s_count);
+    if (idx->leaves) cudaFreeAsync(idx->leaves, ctx->s_count);
+    if (idx->root) cudaFreeAsync(idx->root, ctx->s_count);
+    cudaEventDestroy(idx->ev_train0);
     cudaEventDestroy(idx->ev_start);
     cudaEventDestroy(idx->ev_h2d);
     cudaEventDestroy(idx->ev_ready);
@@ -244,11 +249,17 @@ int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, c
     if (n > 0xffffffffull) return fail(SJCS_ERR_INVALID, "too many particles for one index (%llu)", (unsigned long long)n);
     sjcs_index_opts o{};
     if (opts) o = *opts;
-    if (o.kind != SJCS_INDEX_GRID) return fail(SJCS_ERR_INVALID, "unsupported index kind %d", o.kind);
-    for (int i = 0; i < 4; ++i)
+    if (o.kind != SJCS_INDEX_GRID && o.kind != SJCS_INDEX_LEARNED && o.kind != SJCS_INDEX_MORTON)
+        return fail(SJCS_ERR_INVALID, "unsupported index kind %d", o.kind);
+    for (int i = 0; i < 3; ++i)
         if (o.reserved[i]) return fail(SJCS_ERR_INVALID, "reserved option fields must be zero");
+    if (o.flags & ~(uint32_t)SJCS_INDEX_VERIFY) return fail(SJCS_ERR_INVALID, "unknown index flags 0x%x", o.flags);
     if (!(o.radius_hint >= 0.0f)) return fail(SJCS_ERR_INVALID, "radius_hint must be >= 0");
-    if ((o.grid[0] || o.grid[1] || o.grid[2]) &&
+    const bool morton = o.kind != SJCS_INDEX_GRID;
+    if (morton && (o.grid[0] > (uint32_t)kMaxMortonLevel || o.grid[1] || o.grid[2]))
+        return fail(SJCS_ERR_INVALID, "Morton index: grid[0] is the cell level (0 = automatic, 1..%d), grid[1] and grid[2] must be zero",
+                    kMaxMortonLevel);
+    if (!morton && (o.grid[0] || o.grid[1] || o.grid[2]) &&
         (!o.grid[0] || !o.grid[1] || !o.grid[2] || o.grid[0] > 65535 || o.grid[1] > 65535 || o.grid[2] > 65535 ||
          (uint64_t)o.grid[0] * o.grid[1] * o.grid[2] > (1ull << 31)))
         return fail(SJCS_ERR_INVALID, "grid must be all zero or three values in [1,65535] with <= 2^31 cells");
@@ -280,8 +291,14 @@ int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, c
         idx->had_h2d = true;
     }
     cudaEventRecord(idx->ev_h2d, s);
-    const GridGeom g = auto_grid(n, o.radius_hint, o.grid);
-    rc = build_grid_index(ctx, d_xyz, n, g, idx, s);
+    if (morton) {
+        const int level = o.grid[0] ? (int)o.grid[0] : morton_auto_level(n, o.radius_hint);
+        rc = build_morton_index(ctx, d_xyz, n, level, o.kind == SJCS_INDEX_LEARNED,
+                                (o.flags & SJCS_INDEX_VERIFY) != 0, idx, s);
+    } else {
+        const GridGeom g = auto_grid(n, o.radius_hint, o.grid);
+        rc = build_grid_index(ctx, d_xyz, n, g, idx, s);
+    }
     if (rc) {
         free_index(idx);
         return rc;
@@ -465,6 +482,30 @@ int sjcs_index_grid(const sjcs_index* idx, uint32_t out[3]) {
     return SJCS_OK;
 }
 
+int sjcs_index_learned_info(sjcs_index* idx, sjcs_learned_info* out) {
+    if (!valid_index(idx) || !out) return fail(SJCS_ERR_INVALID, "invalid argument");
+    if (idx->kind != SJCS_INDEX_LEARNED) return fail(SJCS_ERR_INVALID, "not a learned index");
+    int rc = set_device(idx->ctx);
+    if (rc) return rc;
+    SJCS_CUDA_TRY(cudaEventSynchronize(idx->ev_ready));
+    LearnedRoot r{};
+    SJCS_CUDA_TRY(cudaMemcpy(&r, idx->root, sizeof(r), cudaMemcpyDeviceToHost));
+    sjcs_learned_info info{};
+    info.level = (uint32_t)idx->level;
+    info.leaves = kLeaves;
+    info.nonempty = r.nonempty;
+    info.max_err = r.max_err;
+    info.mean_err = r.nonempty ? (double)r.sum_err / (double)r.nonempty : 0.0;
+    info.checked = r.checked;
+    info.mismatches = r.mismatches;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, idx->ev_h2d, idx->ev_train0) == cudaSuccess) info.sort_ms = ms;
+    if (cudaEventElapsedTime(&ms, idx->ev_train0, idx->ev_ready) == cudaSuccess) info.train_ms = ms;
+    cudaGetLastError();
+    *out = info;
+    return SJCS_OK;
+}
+
 int sjcs_index_timing(const sjcs_index* idx, sjcs_timing* out) {
     if (!valid_index(idx) || !out) return fail(SJCS_ERR_INVALID, "invalid argument");
     SJCS_CUDA_TRY(cudaEventSynchronize(idx->ev_ready));
@@ -552,7 +593,7 @@ int sjcs_query_count(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx) {
     q->count_events.push_back(e0);
     q->count_events.push_back(e1);
     cudaEventRecord(e0, s);
-    rc = launch_shell_count(ctx, q, idx, s);
+    rc = idx->kind == SJCS_INDEX_GRID ? launch_shell_count(ctx, q, idx, s) : launch_morton_count(ctx, q, idx, s);
     cudaEventRecord(e1, s);
     cudaEventRecord(q->ev_last, s);
     return rc;

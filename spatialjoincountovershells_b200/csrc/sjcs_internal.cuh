@@ -121,15 +121,24 @@ struct sjcs_ctx {
     std::mutex mu;
 };
 
+namespace sjcs {
+struct LearnedLeaf;
+struct LearnedRoot;
+}
+
 struct sjcs_index {
     uint32_t magic;
     sjcs_ctx* ctx;
     int kind;
     uint64_t n;
-    sjcs::GridGeom geom;
+    sjcs::GridGeom geom;   // grid kind
     float4* pts;           // n sorted particles
-    uint32_t* cell_start;  // geom.ncells + 1 entries
-    cudaEvent_t ev_start, ev_h2d, ev_ready;
+    uint32_t* cell_start;  // grid: geom.ncells + 1 entries; Morton kinds: 8^level + 1 entries
+    int level;             // Morton kinds: cell level of the offset table and of the lookups
+    bool verify;           // learned kind: the model was checked against the table
+    sjcs::LearnedLeaf* leaves;  // learned kind: 4096 leaves
+    sjcs::LearnedRoot* root;    // learned kind: root model and training statistics
+    cudaEvent_t ev_start, ev_h2d, ev_ready, ev_train0;  // ev_train0: sort done, training starts
     bool had_h2d;
 };
 
@@ -172,6 +181,14 @@ constexpr uint32_t kQueryMagic = 0x534a5158u;  // "SJQX"
 int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGeom& g,
                      sjcs_index* idx, cudaStream_t s);
 GridGeom auto_grid(uint64_t n, float radius_hint, const uint32_t* grid_req);
+
+// learned_index.cu: Morton kinds (plain Morton offset table, learned rank model)
+int morton_auto_level(uint64_t n, float radius_hint);
+int build_morton_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, int level, bool learned, bool verify,
+                       sjcs_index* idx, cudaStream_t s);
+
+// morton_count.cu
+int launch_morton_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s);
 
 // query_prep.cu
 int sort_halos(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride_bytes, uint64_t nhalos,
