@@ -64,6 +64,13 @@ extern "C" {
                                    every cell boundary with the offset table; on any mismatch the
                                    index answers from the table */
 
+/* count schedules: how the count kernel hands halos to warps */
+#define SJCS_SCHED_AUTO    0 /* the context's autotuned choice for this workload shape, else STATIC */
+#define SJCS_SCHED_STATIC  1 /* warps take halos strided over the Morton order, in batches of 32 */
+#define SJCS_SCHED_QUEUE   2 /* persistent warps pull work from a queue ordered by estimated candidate
+                                count (largest first); heavy halos are split into pieces that several
+                                warps count together (grid index only; other kinds count STATIC) */
+
 /* query flags */
 #define SJCS_QUERY_PERIODIC     0x1 /* periodic images, as multiRangeCountWithPriodicBoundArraySTR */
 #define SJCS_QUERY_NONPERIODIC  0x0 /* single image, as multiRangeCountArraySTR (MultiRangeCount.c:75-83) */
@@ -109,6 +116,17 @@ typedef struct sjcs_timing {
     float d2h_ms;         /* device-to-host read-back (widening kernel + copy) */
     uint32_t count_calls; /* number of sjcs_query_count calls summed in count_ms */
 } sjcs_timing;
+
+/* A count schedule.  Zero fields take the defaults. */
+typedef struct sjcs_schedule {
+    int      mode;        /* SJCS_SCHED_* */
+    uint32_t piece;       /* queue: candidates per piece of a heavy halo, i.e. the work one warp
+                             takes at a time (rounded up to a power of two; 0 = 8192) */
+    uint32_t max_pieces;  /* queue: most warps counting one halo together (0 = 64) */
+    uint32_t single;      /* queue: estimated candidates from which a halo is a queue item of its
+                             own; lighter halos share items, up to 32 halos and about `piece`
+                             candidates per item (power of two; 0 = piece/8) */
+} sjcs_schedule;
 
 /* ---- errors / version ---------------------------------------------------- */
 
@@ -233,6 +251,26 @@ int sjcs_query_reset(sjcs_ctx *ctx, sjcs_query *q);
  * reset, and the last read-back time (blocks until those are done). */
 int sjcs_query_timing(const sjcs_query *q, sjcs_timing *out);
 int sjcs_query_destroy(sjcs_query *q);
+
+/* ---- schedules and autotuning (no counterpart in the reference, whose
+ * threads take halos in chunks of 100 from a shared counter,
+ * src/astr_rcount/main.c:802-823) ---------------------------------------- */
+
+/* Schedule used by later sjcs_query_count calls on q (default SJCS_SCHED_AUTO).
+ * The schedule changes only how work is spread over warps, never the counts. */
+int sjcs_query_set_schedule(sjcs_ctx *ctx, sjcs_query *q, const sjcs_schedule *sched);
+int sjcs_query_get_schedule(const sjcs_query *q, sjcs_schedule *out);
+/* Time every candidate schedule (static; queue with pieces of 2048, 8192,
+ * 32768 and 131072 candidates and up to 64 warps per halo; queue with pieces
+ * of 32768 and up to 256 warps per halo) on the full query against
+ * idx, keep the fastest on q and remember it in the context for queries of
+ * the same shape (index kind, particles and halos to the nearest power of
+ * two, largest radius, shells, periodicity), where SJCS_SCHED_AUTO finds it.
+ * The query's counts are left as they were.  Blocks; trial_ms[i] (up to
+ * max_trials entries, may be NULL) receives each trial's kernel time in the
+ * order above and *ntrials their number. */
+int sjcs_autotune(sjcs_ctx *ctx, sjcs_query *q, const sjcs_index *idx, sjcs_schedule *chosen,
+                  float *trial_ms, int max_trials, int *ntrials);
 
 /* ---- one-shot, reference semantics --------------------------------------- */
 

@@ -24,6 +24,9 @@ from ._native import (  # noqa: F401
     INDEX_VERIFY,
     QUERY_NONPERIODIC,
     QUERY_PERIODIC,
+    SCHED_AUTO,
+    SCHED_QUEUE,
+    SCHED_STATIC,
     Context,
     Index,
     Query,

@@ -18,6 +18,9 @@ INDEX_MORTON = 2
 INDEX_VERIFY = 0x1
 QUERY_NONPERIODIC = 0
 QUERY_PERIODIC = 1
+SCHED_AUTO = 0
+SCHED_STATIC = 1
+SCHED_QUEUE = 2
 
 # The reference's Halo struct (include/Gadget/BufHalo.h:26-30), 24 bytes.
 HALO_DTYPE = np.dtype([("id", "<u8"), ("mass", "<f4"), ("point", "<f4", (3,))], align=False)
@@ -47,6 +50,10 @@ class sjcs_learned_info(_c.Structure):
     _fields_ = [("level", _c.c_uint32), ("leaves", _c.c_uint32), ("nonempty", _c.c_uint32),
                 ("max_err", _c.c_uint32), ("mean_err", _c.c_double), ("checked", _c.c_uint64),
                 ("mismatches", _c.c_uint64), ("sort_ms", _c.c_float), ("train_ms", _c.c_float)]
+
+
+class sjcs_schedule(_c.Structure):
+    _fields_ = [("mode", _c.c_int), ("piece", _c.c_uint32), ("max_pieces", _c.c_uint32), ("single", _c.c_uint32)]
 
 
 class sjcs_timing(_c.Structure):
@@ -79,6 +86,10 @@ _SIGS = {
     "sjcs_index_size": (_c.c_int, [_vp, _c.POINTER(_u64)]),
     "sjcs_index_grid": (_c.c_int, [_vp, _c.POINTER(_c.c_uint32)]),
     "sjcs_index_learned_info": (_c.c_int, [_vp, _c.POINTER(sjcs_learned_info)]),
+    "sjcs_query_set_schedule": (_c.c_int, [_vp, _vp, _c.POINTER(sjcs_schedule)]),
+    "sjcs_query_get_schedule": (_c.c_int, [_vp, _c.POINTER(sjcs_schedule)]),
+    "sjcs_autotune": (_c.c_int, [_vp, _vp, _vp, _c.POINTER(sjcs_schedule), _c.POINTER(_c.c_float), _c.c_int,
+                                 _c.POINTER(_c.c_int)]),
     "sjcs_index_timing": (_c.c_int, [_vp, _c.POINTER(sjcs_timing)]),
     "sjcs_index_destroy": (_c.c_int, [_vp]),
     "sjcs_query_create": (_c.c_int, [_vp, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _pp]),
@@ -263,6 +274,14 @@ class Context:
             keep = arr
         return Index(self, h, keep)
 
+    def autotune(self, query: "Query", index: "Index") -> dict:
+        """Time the candidate count schedules on the full query; keep the fastest."""
+        ch = sjcs_schedule()
+        ms = (_c.c_float * 16)()
+        nt = _c.c_int()
+        _check(lib().sjcs_autotune(self._h, query._h, index._h, _c.byref(ch), ms, 16, _c.byref(nt)))
+        return {"chosen": _sched_dict(ch), "trial_ms": [ms[i] for i in range(nt.value)]}
+
     def query(self, halos, r2, periodic: bool = True) -> "Query":
         """Halo set + squared-radius table.  halos: (n,3) float32, a HALO_DTYPE array
         (its .point field is read in place with stride 24), or a CUDA tensor."""
@@ -376,6 +395,16 @@ class Query:
     def reset(self) -> None:
         _check(lib().sjcs_query_reset(self.ctx._h, self._h))
 
+    def set_schedule(self, mode: int = SCHED_AUTO, piece: int = 0, max_pieces: int = 0, single: int = 0) -> "Query":
+        sc = sjcs_schedule(mode, piece, max_pieces, single)
+        _check(lib().sjcs_query_set_schedule(self.ctx._h, self._h, _c.byref(sc)))
+        return self
+
+    def schedule(self) -> dict:
+        sc = sjcs_schedule()
+        _check(lib().sjcs_query_get_schedule(self._h, _c.byref(sc)))
+        return _sched_dict(sc)
+
     def timing(self) -> dict:
         t = sjcs_timing()
         _check(lib().sjcs_query_timing(self._h, _c.byref(t)))
@@ -392,6 +421,10 @@ class Query:
                 lib().sjcs_query_destroy(self._h)
         except Exception:
             pass
+
+
+def _sched_dict(sc) -> dict:
+    return {f: getattr(sc, f) for f, _ in sjcs_schedule._fields_}
 
 
 def launch_counter() -> int:

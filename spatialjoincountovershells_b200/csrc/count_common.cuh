@@ -151,5 +151,56 @@ __device__ __forceinline__ void run_rows(const CountParams& p, const Image& im, 
     }
 }
 
+// Piece `part` of `nparts` of the candidates of the lanes' rows: the
+// contiguous share [total*part/nparts, total*(part+1)/nparts) of the
+// flattened candidate sequence, so nparts warps sharing a halo split every
+// row set evenly and together test each candidate once.
+template <int BIN, bool BIG>
+__device__ __forceinline__ void run_rows_part(const CountParams& p, const Image& im, uint32_t start, uint32_t end,
+                                              uint32_t* __restrict__ sink, const float* __restrict__ tab,
+                                              const uint32_t* __restrict__ lut, int lane, uint32_t part,
+                                              uint32_t nparts) {
+    const uint32_t len = end - start;
+    uint32_t incl = len;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += v;
+    }
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    const uint32_t off = start - (incl - len);
+    const uint32_t tb = (uint32_t)(((uint64_t)total * part) / nparts);
+    const uint32_t te = (uint32_t)(((uint64_t)total * (part + 1u)) / nparts);
+    for (uint32_t wb = tb; wb < te; wb += 64) {
+        const uint32_t t0 = wb + (uint32_t)lane, t1 = t0 + 32u;
+        int r0 = 0, r1 = 0;
+#pragma unroll
+        for (int b = 16; b >= 1; b >>= 1) {
+            const uint32_t v0 = __shfl_sync(0xffffffffu, incl, r0 + b - 1);
+            const uint32_t v1 = __shfl_sync(0xffffffffu, incl, r1 + b - 1);
+            r0 += (v0 <= t0) ? b : 0;
+            r1 += (v1 <= t1) ? b : 0;
+        }
+        const uint32_t o0 = __shfl_sync(0xffffffffu, off, r0);
+        const uint32_t o1 = __shfl_sync(0xffffffffu, off, r1);
+        const bool l0 = t0 < te, l1 = t1 < te;
+        const float4 p0 = l0 ? __ldg(p.pts + (t0 + o0)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 p1 = l1 ? __ldg(p.pts + (t1 + o1)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        test_candidate<BIN, BIG>(p, im, p0, l0, sink, tab, lut);
+        test_candidate<BIN, BIG>(p, im, p1, l1, sink, tab, lut);
+    }
+}
+
+// Shell bucket of an estimated candidate count, for ordering work by size:
+// 0 for none, else 1 + 8*floor(log2 e) + the next 3 bits of e (<= 256 values;
+// neighbouring buckets differ by a factor <= 2^(1/8)).
+__device__ __forceinline__ uint32_t est_bucket(uint32_t e) {
+    if (e == 0) return 0u;
+    const int lg = 31 - __clz(e);
+    const uint32_t mant = lg >= 3 ? (e >> (lg - 3)) & 7u : (e << (3 - lg)) & 7u;
+    const uint32_t b = 1u + 8u * (uint32_t)lg + mant;
+    return b < 255u ? b : 255u;  // 8 bits
+}
+
 }  // namespace count
 }  // namespace sjcs

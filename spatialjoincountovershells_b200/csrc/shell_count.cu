@@ -38,6 +38,7 @@
 // back before the square root; the x cell range then uses cx -+ (xr + 1e-3 +
 // 1e-6*(|cx| + xr)).
 #include "count_common.cuh"
+#include "radix_sort.cuh"
 #include "sjcs_internal.cuh"
 
 namespace sjcs {
@@ -132,12 +133,30 @@ __device__ __forceinline__ void count_image(const CountParams& p, const Image& i
     }
 }
 
+// Piece `part` of `nparts` of every row chunk of an image (heavy halos
+// shared by several warps).
+template <int BIN, bool BIG>
+__device__ __forceinline__ void count_image_part(const CountParams& p, const Image& im,
+                                                 uint32_t* __restrict__ sink, const float* __restrict__ tab,
+                                                 const uint32_t* __restrict__ lut, int lane, uint32_t part,
+                                                 uint32_t nparts) {
+    float gy, gz;
+    gap_tables(p, im, lane, &gy, &gz);
+    for (uint32_t rb = 0; rb < im.nrows; rb += 32u) {
+        uint32_t s0, s1;
+        row_issue(p, im, rb, lane, gy, gz, &s0, &s1);
+        run_rows_part<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane, part, nparts);
+    }
+}
+
 // Periodic images other than the un-shifted one: every non-empty subset S of
-// the flagged axes (MultiRangeCount.c:31-71).
+// the flagged axes (MultiRangeCount.c:31-71).  nparts > 1: this warp's piece
+// of each image only.
 template <int BIN, bool BIG>
 __device__ __forceinline__ void count_shifted_images(const CountParams& p, const float4 c,
                                                      uint32_t* __restrict__ sink, const float* __restrict__ tab,
-                                                     const uint32_t* __restrict__ lut, int lane) {
+                                                     const uint32_t* __restrict__ lut, int lane,
+                                                     uint32_t part = 0, uint32_t nparts = 1) {
     const float lox = __fsub_rn(c.x, p.half), hix = __fadd_rn(c.x, p.half);
     const float loy = __fsub_rn(c.y, p.half), hiy = __fadd_rn(c.y, p.half);
     const float loz = __fsub_rn(c.z, p.half), hiz = __fadd_rn(c.z, p.half);
@@ -151,7 +170,8 @@ __device__ __forceinline__ void count_shifted_images(const CountParams& p, const
     const float sz = (loz < kBoxLow) ? __fadd_rn(c.z, kBoxUpp) : __fsub_rn(c.z, kBoxUpp);
     for (unsigned S = F; S != 0; S = (S - 1u) & F) {
         const Image im = make_image(p, (S & 1u) ? sx : c.x, (S & 2u) ? sy : c.y, (S & 4u) ? sz : c.z);
-        count_image<BIN, BIG>(p, im, 0, sink, tab, lut, lane);
+        if (nparts > 1) count_image_part<BIN, BIG>(p, im, sink, tab, lut, lane, part, nparts);
+        else count_image<BIN, BIG>(p, im, 0, sink, tab, lut, lane);
     }
 }
 
@@ -242,90 +262,286 @@ __device__ __forceinline__ void fetch_rows(const CountParams& p, const WarpPlans
     *s1 = b;
 }
 
-// Each warp takes batches of 32 of its halos.  Planning runs one lane per
-// halo; execution runs the whole warp on one halo at a time over its planned
-// rows, while the cell-table loads of the next halo of the batch are in
-// flight.  Halos with more than 28 rows and the shifted periodic images
+// Flush a warp's shared counters into the halo's count row (fire-and-forget
+// reductions) and clear them.
+__device__ __forceinline__ void flush_counts(const CountParams& p, uint32_t* __restrict__ wcnt,
+                                             uint32_t* __restrict__ row, int lane) {
+    __syncwarp();
+    for (int sh = lane; sh < p.nrads; sh += 32) {
+        const uint32_t v = wcnt[sh];
+        if (v) {
+            wcnt[sh] = 0u;
+            atomicAdd(row + sh, v);  // result unused: compiles to a reduction
+        }
+    }
+    __syncwarp();
+}
+
+// One batch of nb <= 32 halos (halo k = c_lane of lane k).  Planning runs one
+// lane per halo; execution runs the whole warp on one halo at a time over its
+// planned rows, while the cell-table loads of the next halo of the batch are
+// in flight.  Halos with more than 28 rows and the shifted periodic images
 // (about 3% of halos at the workload's sizes) are counted in place.
 template <int BIN, bool BIG>
-__global__ void __launch_bounds__(CT_THREADS, 8) k_shell_count(CountParams p) {
-    extern __shared__ uint32_t smem[];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    WarpPlans* wp = reinterpret_cast<WarpPlans*>(smem) + warp;
+__device__ __forceinline__ void count_batch(const CountParams& p, WarpPlans* wp, uint32_t nb, float4 c_lane,
+                                            uint32_t* __restrict__ wcnt, const float* __restrict__ tab,
+                                            const uint32_t* __restrict__ lut, int lane) {
+    {
+        const bool valid = (uint32_t)lane < nb;
+        plan_halo(p, c_lane, valid, &wp->plan[lane], wp->row_cell[lane], wp->row_len[lane]);
+    }
+    __syncwarp();
+    uint32_t s0, s1;
+    {
+        const uint32_t n0 = wp->plan[0].nrows;
+        fetch_rows(p, wp, 0, n0 == kSlowPlan ? 0u : n0, lane, &s0, &s1);
+    }
+    for (uint32_t k = 0; k < nb; ++k) {
+        const HaloPlan pl = wp->plan[k];
+        // the next halo's row loads overlap this halo's tests
+        uint32_t t0 = 0, t1 = 0;
+        if (k + 1 < nb) {
+            const uint32_t nn = wp->plan[k + 1].nrows;
+            fetch_rows(p, wp, k + 1, nn == kSlowPlan ? 0u : nn, lane, &t0, &t1);
+        }
+        uint32_t* row = p.counts + (uint64_t)pl.row * (uint64_t)p.nrads;
+        uint32_t* sink = BIG ? row : wcnt;
+        Image im;
+        im.cx = pl.cx;
+        im.cy = pl.cy;
+        im.cz = pl.cz;
+        im.lox = pl.lox;
+        im.hix = pl.hix;
+        im.loy = pl.loy;
+        im.hiy = pl.hiy;
+        im.loz = pl.loz;
+        im.hiz = pl.hiz;
+        if (pl.nrows == kSlowPlan) {
+            count_image<BIN, BIG>(p, make_image(p, pl.cx, pl.cy, pl.cz), 0, sink, tab, lut, lane);
+        } else {
+            run_rows<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane);
+        }
+        if (pl.flags) count_shifted_images<BIN, BIG>(p, make_float4(pl.cx, pl.cy, pl.cz, 0.f), sink, tab, lut, lane);
+        if (!BIG) flush_counts(p, wcnt, row, lane);
+        s0 = t0;
+        s1 = t1;
+    }
+    __syncwarp();  // the batch's plans are read before the next batch overwrites them
+}
+
+// Shared-memory set-up common to both schedules: per-warp plans, the r2
+// table, the shell lookup table and per-warp counters.
+struct SmemView {
+    WarpPlans* wp;
+    const float* tab;
+    const uint32_t* lut;
+    uint32_t* wcnt;
+};
+
+template <bool BIG>
+__device__ __forceinline__ SmemView setup_smem(const CountParams& p, uint32_t* smem, int tid, int warp) {
+    SmemView v;
+    v.wp = reinterpret_cast<WarpPlans*>(smem) + warp;
     float* r2s = reinterpret_cast<float*>(reinterpret_cast<WarpPlans*>(smem) + CT_WARPS);
     uint32_t* luts = reinterpret_cast<uint32_t*>(r2s + p.pad);
-    uint32_t* wcnt = luts + p.nlut + warp * p.nrads;
+    v.wcnt = luts + p.nlut + warp * p.nrads;
     if (!BIG) {
         for (int i = tid; i < p.pad; i += CT_THREADS) r2s[i] = p.r2[i];
         for (int i = tid; i < p.nlut; i += CT_THREADS) luts[i] = p.lut[i];
         for (int i = tid; i < CT_WARPS * p.nrads; i += CT_THREADS) luts[p.nlut + i] = 0u;
     }
+    v.tab = BIG ? p.r2 : r2s;
+    v.lut = BIG ? p.lut : luts;
+    return v;
+}
+
+// Static schedule: warp gw of W takes halos gw, gw + W, gw + 2W, ... in
+// batches of 32, so at any moment the resident warps work on one contiguous
+// window of the Morton order and share particle lines in L1/L2.
+template <int BIN, bool BIG>
+__global__ void __launch_bounds__(CT_THREADS, 8) k_shell_count(CountParams p) {
+    extern __shared__ uint32_t smem[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const SmemView v = setup_smem<BIG>(p, smem, tid, warp);
     __syncthreads();
-    const float* tab = BIG ? p.r2 : r2s;
-    const uint32_t* lut = BIG ? p.lut : luts;
-    // Warp gw of W takes halos gw, gw + W, gw + 2W, ... in batches of 32, so
-    // at any moment the resident warps work on one contiguous window of the
-    // Morton order and share particle lines in L1/L2.
     const uint64_t W = (uint64_t)gridDim.x * CT_WARPS;
     const uint64_t gw = (uint64_t)blockIdx.x * CT_WARPS + warp;
     const uint64_t mine = p.nhalos > gw ? (p.nhalos - gw + W - 1) / W : 0;  // halos of this warp
-
     for (uint64_t b0 = 0; b0 < mine; b0 += kBatch) {
         const uint32_t nb = (uint32_t)min((uint64_t)kBatch, mine - b0);
-        {
-            const bool valid = (uint32_t)lane < nb;
-            const float4 c = valid ? p.halos[(b0 + lane) * W + gw] : make_float4(0.f, 0.f, 0.f, 0.f);
-            plan_halo(p, c, valid, &wp->plan[lane], wp->row_cell[lane], wp->row_len[lane]);
-        }
-        __syncwarp();
-        uint32_t s0, s1;
-        {
-            const uint32_t n0 = wp->plan[0].nrows;
-            fetch_rows(p, wp, 0, n0 == kSlowPlan ? 0u : n0, lane, &s0, &s1);
-        }
-        for (uint32_t k = 0; k < nb; ++k) {
-            const HaloPlan pl = wp->plan[k];
-            // the next halo's row loads overlap this halo's tests
-            uint32_t t0 = 0, t1 = 0;
-            if (k + 1 < nb) {
-                const uint32_t nn = wp->plan[k + 1].nrows;
-                fetch_rows(p, wp, k + 1, nn == kSlowPlan ? 0u : nn, lane, &t0, &t1);
-            }
-            uint32_t* row = p.counts + (uint64_t)pl.row * (uint64_t)p.nrads;
-            uint32_t* sink = BIG ? row : wcnt;
-            Image im;
-            im.cx = pl.cx;
-            im.cy = pl.cy;
-            im.cz = pl.cz;
-            im.lox = pl.lox;
-            im.hix = pl.hix;
-            im.loy = pl.loy;
-            im.hiy = pl.hiy;
-            im.loz = pl.loz;
-            im.hiz = pl.hiz;
-            if (pl.nrows == kSlowPlan) {
-                count_image<BIN, BIG>(p, make_image(p, pl.cx, pl.cy, pl.cz), 0, sink, tab, lut, lane);
-            } else {
-                run_rows<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane);
-            }
-            if (pl.flags) count_shifted_images<BIN, BIG>(p, make_float4(pl.cx, pl.cy, pl.cz, 0.f), sink, tab, lut, lane);
-            if (!BIG) {
-                __syncwarp();
-                for (int sh = lane; sh < p.nrads; sh += 32) {
-                    const uint32_t v = wcnt[sh];
-                    if (v) {
-                        wcnt[sh] = 0u;
-                        atomicAdd(row + sh, v);  // result unused: compiles to a reduction
-                    }
-                }
-                __syncwarp();
-            }
-            s0 = t0;
-            s1 = t1;
-        }
-        __syncwarp();  // the batch's plans are read before the next batch overwrites them
+        const float4 c = (uint32_t)lane < nb ? p.halos[(b0 + lane) * W + gw] : make_float4(0.f, 0.f, 0.f, 0.f);
+        count_batch<BIN, BIG>(p, v.wp, nb, c, v.wcnt, v.tab, v.lut, lane);
     }
 }
+
+// ---- persistent work-queue schedule -----------------------------------------
+//
+// k_estimate    per halo (Morton order): the number of candidates of its
+//               clipped rows (times 2^k for k flagged periodic axes) and its
+//               size bucket (est_bucket, 8 bits); a histogram of the buckets
+// sort          one 8-bit radix pass by descending bucket (stable: Morton
+//               order within a bucket) -> ord[i] = Morton index
+// k_plan_items  per bucket (lower bound e of its estimates): halos with
+//               e >= piece are split into min(max_pieces, ceil(e/piece))
+//               pieces that separate warps count (every row set split
+//               evenly); halos with e >= single are items of their own;
+//               lighter halos go min(32, piece/e) to an item.  The buckets'
+//               item counts are prefix-summed into a 256-entry table.
+// k_queue       persistent warps claim items with one atomicAdd each (no
+//               claim ever fails or retries), largest buckets first, so the
+//               longest items start early and the light ones fill the tail.
+
+struct BucketPlan {
+    uint32_t start;   // first position of the bucket in ord
+    uint32_t count;   // halos in the bucket
+    uint32_t per;     // halos per item (batch) or 0 when halos are split
+    uint32_t pieces;  // pieces per halo when split
+    uint32_t item0;   // first item of the bucket
+};
+constexpr int kBuckets = 256;
+
+struct QueueParams {
+    const uint32_t* __restrict__ ord;     // Morton index, descending size buckets
+    const BucketPlan* __restrict__ plan;  // [kBuckets] in position order (key 0 = largest)
+    uint32_t* __restrict__ ctl;           // [0] item counter, [1] total items
+};
+
+__device__ __forceinline__ uint32_t bucket_low(uint32_t b) {
+    if (b == 0) return 0u;
+    const uint32_t lg = (b - 1u) >> 3, mant = (b - 1u) & 7u;
+    return lg >= 3 ? (8u + mant) << (lg - 3) : (8u + mant) >> (3 - lg);
+}
+
+__global__ void k_estimate(CountParams p, uint32_t* __restrict__ key, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t sh[kBuckets];
+    for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) sh[i] = 0;
+    __syncthreads();
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < p.nhalos) {
+        const float4 c = p.halos[i];
+        const Image im = make_image(p, c.x, c.y, c.z);
+        uint32_t e;
+        if (im.nrows > 4096u) {
+            e = 0x40000000u;  // far too many rows to walk here: certainly heavy
+        } else {
+            uint64_t sum = 0;
+            for (int zz = im.z0; zz <= im.z1; ++zz) {
+                const float gz = p.prune ? cell_gap(im.cz, zz, p.h[2], p.g.G[2]) : 0.0f;
+                const float rz = __fsub_rn(p.r2p, __fmul_rn(gz, gz));
+                for (int yy = im.y0; yy <= im.y1; ++yy) {
+                    int xa = im.x0, xb = im.x1;
+                    if (p.prune) {
+                        const float gy = cell_gap(im.cy, yy, p.h[1], p.g.G[1]);
+                        const float rem = __fadd_rn(__fsub_rn(rz, __fmul_rn(gy, gy)), p.r2slack);
+                        if (rem < 0.0f) continue;
+                        float xr = rem > 0.0f ? __fmul_rn(rem, rsqrtf(rem)) : 0.0f;
+                        xr = __fadd_rn(xr, 1e-3f + 1e-6f * (fabsf(im.cx) + xr));
+                        xa = max(xa, cell_of(__fsub_rn(im.cx, xr), p.g.inv_h[0], p.g.G[0]));
+                        const float xh = __fadd_rn(im.cx, xr);
+                        if (xh == xh) xb = min(xb, cell_of(xh, p.g.inv_h[0], p.g.G[0]));
+                    }
+                    if (xa > xb) continue;
+                    const uint64_t rowcell = ((uint64_t)zz * (uint64_t)p.g.G[1] + (uint64_t)yy) * (uint64_t)p.g.G[0];
+                    sum += __ldg(p.cs + rowcell + xb + 1) - __ldg(p.cs + rowcell + xa);
+                }
+            }
+            if (p.periodic) {
+                const int k = ((im.lox < kBoxLow) | (im.hix > kBoxUpp)) + ((im.loy < kBoxLow) | (im.hiy > kBoxUpp)) +
+                              ((im.loz < kBoxLow) | (im.hiz > kBoxUpp));
+                sum <<= k;
+            }
+            e = sum < 0x40000000ull ? (uint32_t)sum : 0x40000000u;
+        }
+        const uint32_t k = 255u - est_bucket(e);
+        key[i] = k;
+        atomicAdd(&sh[k], 1u);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kBuckets; k += blockDim.x)
+        if (sh[k]) atomicAdd(hist + k, sh[k]);
+}
+
+// One block of kBuckets threads: bucket starts, item sizes and item prefix.
+__global__ void k_plan_items(const uint32_t* __restrict__ hist, uint32_t piece, uint32_t max_pieces,
+                             uint32_t single, BucketPlan* __restrict__ plan, uint32_t* __restrict__ ctl) {
+    __shared__ uint32_t s_cnt[kBuckets], s_items[kBuckets];
+    const int k = threadIdx.x;  // position order: key k holds bucket 255 - k
+    const uint32_t cnt = hist[k];
+    const uint32_t lo = bucket_low(255u - (uint32_t)k);
+    uint32_t per = 0, pieces = 1, items;
+    if (lo >= piece) {
+        pieces = min(max_pieces, (lo + piece - 1u) / piece);
+        items = cnt * pieces;  // <= 2^32 for the sizes accepted (nhalos * max_pieces is checked on the host)
+    } else {
+        per = lo >= single ? 1u : min(32u, max(1u, piece / max(lo, 1u)));
+        items = (cnt + per - 1u) / per;
+    }
+    s_cnt[k] = cnt;
+    s_items[k] = items;
+    __syncthreads();
+    if (k == 0) {
+        uint32_t pos = 0, it = 0;
+        for (int j = 0; j < kBuckets; ++j) {
+            const uint32_t c = s_cnt[j], n = s_items[j];
+            s_cnt[j] = pos;
+            s_items[j] = it;
+            pos += c;
+            it += n;
+        }
+        ctl[0] = 0;
+        ctl[1] = it;
+    }
+    __syncthreads();
+    plan[k] = BucketPlan{s_cnt[k], cnt, per, pieces, s_items[k]};
+}
+
+template <int BIN, bool BIG>
+__global__ void __launch_bounds__(CT_THREADS, 8) k_shell_count_queue(CountParams p, QueueParams q) {
+    extern __shared__ uint32_t smem[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const SmemView v = setup_smem<BIG>(p, smem, tid, warp);
+    __syncthreads();
+    const uint32_t nitems = q.ctl[1];
+    int bk = 0;  // claims only grow, so each warp's bucket search moves forward
+    for (;;) {
+        uint32_t g = 0;
+        if (lane == 0) g = atomicAdd(q.ctl, 1u);
+        g = __shfl_sync(0xffffffffu, g, 0);
+        if (g >= nitems) break;
+        while (bk + 1 < kBuckets && __ldg(&q.plan[bk + 1].item0) <= g) ++bk;
+        const BucketPlan bp = q.plan[bk];
+        const uint32_t r = g - bp.item0;
+        if (bp.per == 0) {
+            const uint32_t pos = bp.start + r / bp.pieces, part = r % bp.pieces;
+            const float4 c = p.halos[q.ord[pos]];
+            uint32_t* row = p.counts + (uint64_t)__float_as_uint(c.w) * (uint64_t)p.nrads;
+            uint32_t* sink = BIG ? row : v.wcnt;
+            const Image im = make_image(p, c.x, c.y, c.z);
+            if (bp.pieces > 1) count_image_part<BIN, BIG>(p, im, sink, v.tab, v.lut, lane, part, bp.pieces);
+            else count_image<BIN, BIG>(p, im, 0, sink, v.tab, v.lut, lane);
+            if (p.periodic) count_shifted_images<BIN, BIG>(p, c, sink, v.tab, v.lut, lane, part, bp.pieces);
+            if (!BIG) flush_counts(p, v.wcnt, row, lane);
+        } else {
+            const uint32_t first = r * bp.per;
+            const uint32_t nb = min(bp.per, bp.count - first);
+            const float4 c = (uint32_t)lane < nb ? p.halos[q.ord[bp.start + first + lane]]
+                                                 : make_float4(0.f, 0.f, 0.f, 0.f);
+            count_batch<BIN, BIG>(p, v.wp, nb, c, v.wcnt, v.tab, v.lut, lane);
+        }
+    }
+}
+
+struct KeyFromEst {
+    const uint32_t* __restrict__ key;
+    __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return key[i]; }
+};
+struct PayIndex {
+    __device__ __forceinline__ uint4 operator()(uint64_t i) const { return make_uint4((uint32_t)i, 0u, 0u, 0u); }
+};
+struct SinkOrd {
+    uint32_t* __restrict__ ord;
+    __device__ __forceinline__ void operator()(uint32_t g, uint32_t, const uint4& v) const { ord[g] = v.x; }
+};
 
 template <int BIN, bool BIG>
 int launch_variant(sjcs_ctx* ctx, const CountParams& p, size_t smem, cudaStream_t s) {
@@ -343,9 +559,44 @@ int launch_variant(sjcs_ctx* ctx, const CountParams& p, size_t smem, cudaStream_
     return SJCS_OK;
 }
 
+template <int BIN, bool BIG>
+int launch_queue(sjcs_ctx* ctx, const CountParams& p, const Schedule& sc, size_t smem, cudaStream_t s) {
+    const uint64_t n = p.nhalos;
+    if (n * (uint64_t)sc.max_pieces >= (1ull << 32))
+        return fail(SJCS_ERR_INVALID, "queue schedule: nhalos * max_pieces must stay below 2^32");
+    const uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+    StreamScratch scr(s);  // freed (stream-ordered) after the kernels below
+    uint32_t *key, *ord, *ctl, *hist, *rhist;
+    BucketPlan* plan;
+    SJCS_CUDA_TRY(scr.alloc(&key, n * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&ord, n * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&ctl, 4 * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&hist, kBuckets * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&plan, kBuckets * sizeof(BucketPlan)));
+    SJCS_CUDA_TRY(scr.alloc(&rhist, (uint64_t)RS_BINS * ntiles * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(cudaMemsetAsync(hist, 0, kBuckets * sizeof(uint32_t), s));
+    k_estimate<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, key, hist);
+    SJCS_LAUNCH_CHECK();
+    int rc = radix_sort_records(n, 8, KeyFromEst{key}, PayIndex{}, SinkOrd{ord}, nullptr, nullptr, nullptr, nullptr,
+                                rhist, s);
+    if (rc) return rc;
+    k_plan_items<<<1, kBuckets, 0, s>>>(hist, sc.piece, sc.max_pieces, sc.single, plan, ctl);
+    SJCS_LAUNCH_CHECK();
+    auto kern = k_shell_count_queue<BIN, BIG>;
+    if (smem > 48 * 1024)
+        SJCS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    SJCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, CT_THREADS, smem));
+    if (per_sm < 1) per_sm = 1;
+    kern<<<(unsigned)(ctx->num_sms * per_sm), CT_THREADS, smem, s>>>(p, QueueParams{ord, plan, ctl});
+    SJCS_LAUNCH_CHECK();
+    return SJCS_OK;
+}
+
 }  // namespace
 
-int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s) {
+int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s,
+                       const Schedule* sc) {
     if (q->nhalos == 0 || idx->n == 0) return SJCS_OK;
     CountParams p;
     p.pts = idx->pts;
@@ -373,6 +624,19 @@ int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx
     if (big) p.nlut = q->nlut;  // table and LUT are read from global memory
     const size_t smem = CT_WARPS * sizeof(WarpPlans) +
                         (big ? 0 : (size_t)(q->pad + q->nlut + CT_WARPS * q->nrads) * sizeof(uint32_t));
+    if (sc && sc->mode == SJCS_SCHED_QUEUE) {
+        switch (bin) {
+            case BIN_LUT:
+                return big ? launch_queue<BIN_LUT, true>(ctx, p, *sc, smem, s)
+                           : launch_queue<BIN_LUT, false>(ctx, p, *sc, smem, s);
+            case BIN_BSEARCH:
+                return big ? launch_queue<BIN_BSEARCH, true>(ctx, p, *sc, smem, s)
+                           : launch_queue<BIN_BSEARCH, false>(ctx, p, *sc, smem, s);
+            default:
+                return big ? launch_queue<BIN_FIRST_MATCH, true>(ctx, p, *sc, smem, s)
+                           : launch_queue<BIN_FIRST_MATCH, false>(ctx, p, *sc, smem, s);
+        }
+    }
     switch (bin) {
         case BIN_LUT:
             return big ? launch_variant<BIN_LUT, true>(ctx, p, smem, s) : launch_variant<BIN_LUT, false>(ctx, p, smem, s);

@@ -5,7 +5,9 @@
 #include <cstdarg>
 #include <cstring>
 #include <new>
+#include <string>
 #include <thread>
+#include <vector>
 
 #include "morton.cuh"
 #include "sjcs_internal.cuh"
@@ -308,6 +310,43 @@ int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, c
     return SJCS_OK;
 }
 
+uint32_t pow2_ceil(uint32_t v) {
+    uint32_t r = 1;
+    while (r < v && r < (1u << 30)) r <<= 1;
+    return r;
+}
+
+// Key of a workload shape for the autotuned-schedule cache.
+std::string shape_key(const sjcs_query* q, const sjcs_index* idx) {
+    auto lg = [](uint64_t v) { int k = 0; while ((1ull << k) < v && k < 63) ++k; return k; };
+    char buf[128];
+    uint32_t rbits;
+    std::memcpy(&rbits, &q->R, sizeof(rbits));
+    std::snprintf(buf, sizeof(buf), "k%d n%d h%d r%08x s%d p%d", idx->kind, lg(idx->n), lg(q->nhalos), rbits,
+                  q->nrads, q->flags & SJCS_QUERY_PERIODIC);
+    return buf;
+}
+
+Schedule resolve(const sjcs_schedule& in) {
+    Schedule sc{};
+    sc.mode = in.mode == SJCS_SCHED_QUEUE ? SJCS_SCHED_QUEUE : SJCS_SCHED_STATIC;
+    sc.piece = pow2_ceil(in.piece ? in.piece : 32768u);
+    sc.max_pieces = in.max_pieces ? in.max_pieces : 64u;
+    sc.single = pow2_ceil(in.single ? in.single : std::max(1u, sc.piece / 8u));
+    return sc;
+}
+
+// The schedule a count call uses (ctx->mu held).
+Schedule schedule_for(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx) {
+    if (idx->kind != SJCS_INDEX_GRID) return resolve(sjcs_schedule{SJCS_SCHED_STATIC, 0, 0, 0});
+    sjcs_schedule sc = q->sched;
+    if (sc.mode == SJCS_SCHED_AUTO) {
+        auto it = ctx->tuned.find(shape_key(q, idx));
+        sc = it != ctx->tuned.end() ? it->second : sjcs_schedule{SJCS_SCHED_STATIC, 0, 0, 0};
+    }
+    return resolve(sc);
+}
+
 }  // namespace
 }  // namespace sjcs
 
@@ -593,10 +632,98 @@ int sjcs_query_count(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx) {
     q->count_events.push_back(e0);
     q->count_events.push_back(e1);
     cudaEventRecord(e0, s);
-    rc = idx->kind == SJCS_INDEX_GRID ? launch_shell_count(ctx, q, idx, s) : launch_morton_count(ctx, q, idx, s);
+    const Schedule sc = schedule_for(ctx, q, idx);
+    rc = idx->kind == SJCS_INDEX_GRID ? launch_shell_count(ctx, q, idx, s, &sc) : launch_morton_count(ctx, q, idx, s);
     cudaEventRecord(e1, s);
     cudaEventRecord(q->ev_last, s);
     return rc;
+}
+
+int sjcs_query_set_schedule(sjcs_ctx* ctx, sjcs_query* q, const sjcs_schedule* sched) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_query(q) || q->ctx != ctx) return fail(SJCS_ERR_STATE, "query does not belong to this context");
+    if (!sched) return fail(SJCS_ERR_INVALID, "schedule is NULL");
+    if (sched->mode < SJCS_SCHED_AUTO || sched->mode > SJCS_SCHED_QUEUE)
+        return fail(SJCS_ERR_INVALID, "unknown schedule mode %d", sched->mode);
+    if (sched->piece > (1u << 30) || sched->single > (1u << 30) || sched->max_pieces > 65536u)
+        return fail(SJCS_ERR_INVALID, "schedule sizes out of range (piece, single <= 2^30, max_pieces <= 65536)");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    q->sched = *sched;
+    return SJCS_OK;
+}
+
+int sjcs_query_get_schedule(const sjcs_query* q, sjcs_schedule* out) {
+    if (!valid_query(q) || !out) return fail(SJCS_ERR_INVALID, "invalid argument");
+    *out = q->sched;
+    return SJCS_OK;
+}
+
+int sjcs_autotune(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx, sjcs_schedule* chosen, float* trial_ms,
+                  int max_trials, int* ntrials) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_query(q) || q->ctx != ctx) return fail(SJCS_ERR_STATE, "query does not belong to this context");
+    if (!valid_index(idx) || idx->ctx != ctx) return fail(SJCS_ERR_STATE, "index does not belong to this context");
+    if (trial_ms && max_trials < 0) return fail(SJCS_ERR_INVALID, "max_trials < 0");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    std::vector<sjcs_schedule> cand{{SJCS_SCHED_STATIC, 0, 0, 0}};
+    if (idx->kind == SJCS_INDEX_GRID) {
+        for (uint32_t pc : {2048u, 8192u, 32768u, 131072u}) cand.push_back(sjcs_schedule{SJCS_SCHED_QUEUE, pc, 64u, 0});
+        cand.push_back(sjcs_schedule{SJCS_SCHED_QUEUE, 32768u, 256u, 0});
+    }
+    std::vector<float> ms(cand.size(), 0.0f);
+    cudaStream_t s = ctx->s_count;
+    SJCS_CUDA_TRY(cudaStreamWaitEvent(s, idx->ev_ready, 0));
+    // trials count into scratch accumulators; the query's own stay untouched
+    uint32_t* saved = q->counts;
+    uint32_t* tmp = nullptr;
+    const size_t bytes = (size_t)q->nhalos * (size_t)q->nrads * sizeof(uint32_t);
+    SJCS_CUDA_TRY(cudaMallocAsync(&tmp, bytes ? bytes : 16, s));
+    q->counts = tmp;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    auto run = [&](const sjcs_schedule& c, float* out_ms) -> int {
+        const Schedule sc = resolve(c);
+        cudaEventRecord(e0, s);
+        int r = idx->kind == SJCS_INDEX_GRID ? launch_shell_count(ctx, q, idx, s, &sc)
+                                             : launch_morton_count(ctx, q, idx, s);
+        cudaEventRecord(e1, s);
+        if (r) return r;
+        if (cudaEventSynchronize(e1) != cudaSuccess) return fail(SJCS_ERR_CUDA, "autotune trial failed");
+        float t = 0.0f;
+        cudaEventElapsedTime(&t, e0, e1);
+        *out_ms = t;
+        return SJCS_OK;
+    };
+    float warm = 0.0f;
+    rc = run(cand[0], &warm);  // warm-up (caches, clocks, lazy module loading)
+    const int reps = warm < 5.0f ? 3 : 1;
+    for (size_t i = 0; i < cand.size() && !rc; ++i) {
+        float best = 0.0f;
+        for (int r = 0; r < reps && !rc; ++r) {
+            float t = 0.0f;
+            rc = run(cand[i], &t);
+            best = (r == 0 || t < best) ? t : best;
+        }
+        ms[i] = best;
+    }
+    q->counts = saved;
+    cudaFreeAsync(tmp, s);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (rc) return rc;
+    size_t bi = 0;
+    for (size_t i = 1; i < cand.size(); ++i)
+        if (ms[i] < ms[bi]) bi = i;
+    q->sched = cand[bi];
+    ctx->tuned[shape_key(q, idx)] = cand[bi];
+    if (chosen) *chosen = cand[bi];
+    if (trial_ms)
+        for (int i = 0; i < max_trials && i < (int)cand.size(); ++i) trial_ms[i] = ms[i];
+    if (ntrials) *ntrials = (int)cand.size();
+    return SJCS_OK;
 }
 
 int sjcs_query_wait(sjcs_query* q) {

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 #include <cstdint>
 #include <cstdio>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -119,6 +120,7 @@ struct sjcs_ctx {
     cudaStream_t s_build;  // particle copies + index builds
     cudaStream_t s_count;  // halo upload/sort, shell counts, count read-back
     std::mutex mu;
+    std::map<std::string, sjcs_schedule> tuned;  // autotuned schedules by workload shape
 };
 
 namespace sjcs {
@@ -170,6 +172,7 @@ struct sjcs_query {
     cudaEvent_t ev_last;                    // end of the last count call
     cudaEvent_t ev_d0, ev_d1;
     float last_d2h_ms;
+    sjcs_schedule sched;  // count schedule (SJCS_SCHED_AUTO by default)
 };
 
 namespace sjcs {
@@ -194,9 +197,16 @@ int launch_morton_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* id
 int sort_halos(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride_bytes, uint64_t nhalos,
                float4* out, cudaStream_t s);
 
-// shell_count.cu
-int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx,
-                       cudaStream_t s);
+// shell_count.cu.  sc == nullptr or mode SJCS_SCHED_STATIC: static
+// schedule; SJCS_SCHED_QUEUE: persistent work queue (allocates scratch).
+struct Schedule {
+    int mode;             // SJCS_SCHED_STATIC or SJCS_SCHED_QUEUE (resolved, never AUTO)
+    uint32_t piece;       // candidates per piece of a heavy halo
+    uint32_t max_pieces;  // most warps sharing one halo
+    uint32_t single;      // estimate (power of two) from which a halo is an item of its own
+};
+int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s,
+                       const Schedule* sc = nullptr);
 
 // scan.cu: exclusive prefix sum of m u32 values, in place.  `partials`
 // (scan_partials_needed(m) u32) may be given; otherwise it is allocated.
