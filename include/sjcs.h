@@ -78,6 +78,7 @@ extern "C" {
 typedef struct sjcs_ctx   sjcs_ctx;   /* one GPU: streams, scratch, tuning cache */
 typedef struct sjcs_index sjcs_index; /* device-resident index over one particle file */
 typedef struct sjcs_query sjcs_query; /* device-resident halos + radius table + u32 count accumulators */
+typedef struct sjcs_step  sjcs_step;  /* one particle file's step (copy, build, count) captured as a CUDA graph */
 
 /* Build options.  Zero-initialised options select an automatic grid for the
  * plain index (sized from n and radius_hint). */
@@ -251,6 +252,29 @@ int sjcs_query_reset(sjcs_ctx *ctx, sjcs_query *q);
  * reset, and the last read-back time (blocks until those are done). */
 int sjcs_query_timing(const sjcs_query *q, sjcs_timing *out);
 int sjcs_query_destroy(sjcs_query *q);
+
+/* ---- captured file steps (no counterpart in the reference: its per-file
+ * step is constructIndexWithSameThreadPool + threadJoin + destructIndex,
+ * src/astr_rcount/main.c:176-243) ---------------------------------------- */
+
+/* Capture one whole file step as a CUDA graph: the copy of n particles from
+ * the PINNED host buffer host_xyz (sjcs_host_alloc), the index build with
+ * `opts`, the count of every halo of q against it (added to q's
+ * accumulators, with q's schedule as resolved now) and the release of the
+ * index.  Nothing runs at creation.  The graph's memory (particles, index,
+ * scratch) is reserved once and reused by every launch. */
+int sjcs_step_create(sjcs_ctx *ctx, sjcs_query *q, const float *host_xyz, uint64_t n,
+                     const sjcs_index_opts *opts, sjcs_step **out);
+/* Replay the step on the current contents of its host buffer (one graph
+ * launch, ordered after all earlier work of the context; later counts and
+ * read-backs of q are ordered after it).  The buffer may be refilled once
+ * sjcs_step_wait has returned. */
+int sjcs_step_launch(sjcs_ctx *ctx, sjcs_step *st);
+int sjcs_step_wait(sjcs_step *st);
+/* Device time of the last launch, in milliseconds (blocks until it is done). */
+int sjcs_step_time(sjcs_step *st, float *ms);
+/* Destroy after the last launch has finished; q must outlive its steps. */
+int sjcs_step_destroy(sjcs_step *st);
 
 /* ---- schedules and autotuning (no counterpart in the reference, whose
  * threads take halos in chunks of 100 from a shared counter,

@@ -86,6 +86,11 @@ _SIGS = {
     "sjcs_index_size": (_c.c_int, [_vp, _c.POINTER(_u64)]),
     "sjcs_index_grid": (_c.c_int, [_vp, _c.POINTER(_c.c_uint32)]),
     "sjcs_index_learned_info": (_c.c_int, [_vp, _c.POINTER(sjcs_learned_info)]),
+    "sjcs_step_create": (_c.c_int, [_vp, _vp, _vp, _u64, _c.POINTER(sjcs_index_opts), _pp]),
+    "sjcs_step_launch": (_c.c_int, [_vp, _vp]),
+    "sjcs_step_wait": (_c.c_int, [_vp]),
+    "sjcs_step_time": (_c.c_int, [_vp, _c.POINTER(_c.c_float)]),
+    "sjcs_step_destroy": (_c.c_int, [_vp]),
     "sjcs_query_set_schedule": (_c.c_int, [_vp, _vp, _c.POINTER(sjcs_schedule)]),
     "sjcs_query_get_schedule": (_c.c_int, [_vp, _c.POINTER(sjcs_schedule)]),
     "sjcs_autotune": (_c.c_int, [_vp, _vp, _vp, _c.POINTER(sjcs_schedule), _c.POINTER(_c.c_float), _c.c_int,
@@ -252,15 +257,7 @@ class Context:
         """Index over particles: host array (n,3) float32, or a CUDA tensor (device path).
         kind: INDEX_GRID (grid = cells per axis), INDEX_MORTON or INDEX_LEARNED (level =
         Morton cell level, 0 = automatic; verify = judge the model against the table)."""
-        opts = sjcs_index_opts()
-        opts.kind = kind
-        opts.radius_hint = float(radius_hint)
-        if grid is not None:
-            for a in range(3):
-                opts.grid[a] = int(grid[a])
-        if kind != INDEX_GRID:
-            opts.grid[0] = int(level)
-        opts.flags = INDEX_VERIFY if verify else 0
+        opts = _make_opts(radius_hint, grid, kind, level, verify)
         h = _vp()
         if _is_cuda(xyz):
             n = xyz.numel() // 3
@@ -274,7 +271,13 @@ class Context:
             keep = arr
         return Index(self, h, keep)
 
-    def autotune(self, query: "Query", index: "Index") -> dict:
+    def step(self, query: "Query", n: int, radius_hint: float = 0.0, kind: int = INDEX_GRID, level: int = 0,
+             verify: bool = False) -> "Step":
+        """A file step (copy, build, count) captured as a CUDA graph over a pinned
+        host buffer of n particles (Step.buffer, an (n, 3) float32 array)."""
+        return Step(self, query, n, _make_opts(radius_hint, None, kind, level, verify))
+
+    def autotune(self, query: "Query", index: "Index") -> "dict":
         """Time the candidate count schedules on the full query; keep the fastest."""
         ch = sjcs_schedule()
         ms = (_c.c_float * 16)()
@@ -308,6 +311,79 @@ class Context:
                                            len(r2), flags, _c.byref(h)))
             keep = arr
         return Query(self, h, n, len(r2), keep)
+
+
+def _make_opts(radius_hint, grid, kind, level, verify) -> sjcs_index_opts:
+    opts = sjcs_index_opts()
+    opts.kind = kind
+    opts.radius_hint = float(radius_hint)
+    if grid is not None:
+        for a in range(3):
+            opts.grid[a] = int(grid[a])
+    if kind != INDEX_GRID:
+        opts.grid[0] = int(level)
+    opts.flags = INDEX_VERIFY if verify else 0
+    return opts
+
+
+class PinnedBuffer:
+    """Page-locked host memory (sjcs_host_alloc) viewed as a numpy array."""
+
+    def __init__(self, shape, dtype=np.float32):
+        self.nbytes = max(1, int(np.prod(shape)) * np.dtype(dtype).itemsize)
+        self._p = _vp()
+        _check(lib().sjcs_host_alloc(self.nbytes, _c.byref(self._p)))
+        buf = (_c.c_char * self.nbytes).from_address(self._p.value)
+        self.array = np.frombuffer(buf, dtype=dtype, count=int(np.prod(shape))).reshape(shape)
+
+    @property
+    def address(self) -> int:
+        return self._p.value
+
+    def free(self) -> None:
+        if self._p:
+            self.array = None
+            lib().sjcs_host_free(self._p)
+            self._p = _vp()
+
+    def __del__(self):
+        try:
+            self.free()
+        except Exception:
+            pass
+
+
+class Step:
+    """One particle file's copy + build + count captured as a CUDA graph."""
+
+    def __init__(self, ctx: "Context", query: "Query", n: int, opts: sjcs_index_opts):
+        self.ctx = ctx
+        self.query = query
+        self.pinned = PinnedBuffer((n, 3))
+        self.buffer = self.pinned.array
+        self._h = _vp()
+        _check(lib().sjcs_step_create(ctx._h, query._h, _vp(self.pinned.address), n, _c.byref(opts),
+                                      _c.byref(self._h)))
+
+    def launch(self) -> "Step":
+        _check(lib().sjcs_step_launch(self.ctx._h, self._h))
+        return self
+
+    def wait(self) -> "Step":
+        _check(lib().sjcs_step_wait(self._h))
+        return self
+
+    def time_ms(self) -> float:
+        ms = _c.c_float()
+        _check(lib().sjcs_step_time(self._h, _c.byref(ms)))
+        return ms.value
+
+    def destroy(self) -> None:
+        if self._h:
+            _check(lib().sjcs_step_destroy(self._h))
+            self._h = None
+        self.buffer = None
+        self.pinned.free()
 
 
 class Index:

@@ -242,13 +242,8 @@ void free_index(sjcs_index* idx) {
     delete idx;
 }
 
-int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, const sjcs_index_opts* opts,
-                       sjcs_index** out) {
-    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
-    if (!out) return fail(SJCS_ERR_INVALID, "out is NULL");
-    *out = nullptr;
-    if (n && !xyz) return fail(SJCS_ERR_INVALID, "xyz is NULL");
-    if (n > 0xffffffffull) return fail(SJCS_ERR_INVALID, "too many particles for one index (%llu)", (unsigned long long)n);
+// Validated copy of the build options.
+int check_opts(const sjcs_index_opts* opts, sjcs_index_opts* o_out) {
     sjcs_index_opts o{};
     if (opts) o = *opts;
     if (o.kind != SJCS_INDEX_GRID && o.kind != SJCS_INDEX_LEARNED && o.kind != SJCS_INDEX_MORTON)
@@ -265,7 +260,32 @@ int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, c
         (!o.grid[0] || !o.grid[1] || !o.grid[2] || o.grid[0] > 65535 || o.grid[1] > 65535 || o.grid[2] > 65535 ||
          (uint64_t)o.grid[0] * o.grid[1] * o.grid[2] > (1ull << 31)))
         return fail(SJCS_ERR_INVALID, "grid must be all zero or three values in [1,65535] with <= 2^31 cells");
-    int rc = set_device(ctx);
+    *o_out = o;
+    return SJCS_OK;
+}
+
+// Queue the build kernels of an index over device particles on stream s.
+int enqueue_build(sjcs_ctx* ctx, sjcs_index* idx, const float* d_xyz, uint64_t n, const sjcs_index_opts& o,
+                  cudaStream_t s) {
+    if (o.kind != SJCS_INDEX_GRID) {
+        const int level = o.grid[0] ? (int)o.grid[0] : morton_auto_level(n, o.radius_hint);
+        return build_morton_index(ctx, d_xyz, n, level, o.kind == SJCS_INDEX_LEARNED,
+                                  (o.flags & SJCS_INDEX_VERIFY) != 0, idx, s);
+    }
+    return build_grid_index(ctx, d_xyz, n, auto_grid(n, o.radius_hint, o.grid), idx, s);
+}
+
+int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, const sjcs_index_opts* opts,
+                       sjcs_index** out) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!out) return fail(SJCS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (n && !xyz) return fail(SJCS_ERR_INVALID, "xyz is NULL");
+    if (n > 0xffffffffull) return fail(SJCS_ERR_INVALID, "too many particles for one index (%llu)", (unsigned long long)n);
+    sjcs_index_opts o{};
+    int rc = check_opts(opts, &o);
+    if (rc) return rc;
+    rc = set_device(ctx);
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(ctx->mu);
     sjcs_index* idx = new_index(ctx);
@@ -293,14 +313,7 @@ int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, c
         idx->had_h2d = true;
     }
     cudaEventRecord(idx->ev_h2d, s);
-    if (morton) {
-        const int level = o.grid[0] ? (int)o.grid[0] : morton_auto_level(n, o.radius_hint);
-        rc = build_morton_index(ctx, d_xyz, n, level, o.kind == SJCS_INDEX_LEARNED,
-                                (o.flags & SJCS_INDEX_VERIFY) != 0, idx, s);
-    } else {
-        const GridGeom g = auto_grid(n, o.radius_hint, o.grid);
-        rc = build_grid_index(ctx, d_xyz, n, g, idx, s);
-    }
+    rc = enqueue_build(ctx, idx, d_xyz, n, o, s);
     if (rc) {
         free_index(idx);
         return rc;
@@ -347,6 +360,52 @@ Schedule schedule_for(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx)
     return resolve(sc);
 }
 
+}  // namespace
+}  // namespace sjcs
+
+struct sjcs_step {
+    uint32_t magic;
+    sjcs_ctx* ctx;
+    sjcs_query* q;
+    cudaGraph_t graph;
+    cudaGraphExec_t exec;
+    cudaEvent_t ev_pre, ev0, ev1;
+    size_t kernels;  // kernel nodes in the graph
+    bool launched;
+};
+
+namespace sjcs {
+namespace {
+constexpr uint32_t kStepMagic = 0x534a5358u;  // "SJSX"
+bool valid_step(const sjcs_step* s) { return s && s->magic == kStepMagic; }
+
+// Stream work of one file step, queued while s_build is capturing.
+int capture_step_body(sjcs_ctx* ctx, sjcs_query* q, const float* host_xyz, uint64_t n, const sjcs_index_opts& o,
+                      sjcs_index* idx, cudaEvent_t join1, cudaEvent_t join2) {
+    cudaStream_t sb = ctx->s_build, sc = ctx->s_count;
+    float* d = nullptr;
+    SJCS_CUDA_TRY(cudaMallocAsync(&d, n * 3 * sizeof(float), sb));
+    SJCS_CUDA_TRY(cudaMemcpyAsync(d, host_xyz, n * 3 * sizeof(float), cudaMemcpyHostToDevice, sb));
+    int rc = enqueue_build(ctx, idx, d, n, o, sb);
+    SJCS_CUDA_TRY(cudaFreeAsync(d, sb));
+    if (rc) return rc;
+    SJCS_CUDA_TRY(cudaEventRecord(join1, sb));
+    SJCS_CUDA_TRY(cudaStreamWaitEvent(sc, join1, 0));
+    const Schedule sched = schedule_for(ctx, q, idx);
+    rc = idx->kind == SJCS_INDEX_GRID ? launch_shell_count(ctx, q, idx, sc, &sched)
+                                      : launch_morton_count(ctx, q, idx, sc);
+    if (idx->pts) SJCS_CUDA_TRY(cudaFreeAsync(idx->pts, sc));
+    if (idx->cell_start) SJCS_CUDA_TRY(cudaFreeAsync(idx->cell_start, sc));
+    if (idx->leaves) SJCS_CUDA_TRY(cudaFreeAsync(idx->leaves, sc));
+    if (idx->root) SJCS_CUDA_TRY(cudaFreeAsync(idx->root, sc));
+    idx->pts = nullptr;
+    idx->cell_start = nullptr;
+    idx->leaves = nullptr;
+    idx->root = nullptr;
+    SJCS_CUDA_TRY(cudaEventRecord(join2, sc));
+    SJCS_CUDA_TRY(cudaStreamWaitEvent(sb, join2, 0));
+    return rc;
+}
 }  // namespace
 }  // namespace sjcs
 
@@ -637,6 +696,136 @@ int sjcs_query_count(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx) {
     cudaEventRecord(e1, s);
     cudaEventRecord(q->ev_last, s);
     return rc;
+}
+
+int sjcs_step_create(sjcs_ctx* ctx, sjcs_query* q, const float* host_xyz, uint64_t n, const sjcs_index_opts* opts,
+                     sjcs_step** out) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_query(q) || q->ctx != ctx) return fail(SJCS_ERR_STATE, "query does not belong to this context");
+    if (!out) return fail(SJCS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!host_xyz || n == 0) return fail(SJCS_ERR_INVALID, "a step needs a host buffer of n >= 1 particles");
+    if (n > 0xffffffffull) return fail(SJCS_ERR_INVALID, "too many particles for one index (%llu)", (unsigned long long)n);
+    sjcs_index_opts o{};
+    int rc = check_opts(opts, &o);
+    if (rc) return rc;
+    rc = set_device(ctx);
+    if (rc) return rc;
+    cudaPointerAttributes pa{};
+    if (cudaPointerGetAttributes(&pa, host_xyz) != cudaSuccess || pa.type != cudaMemoryTypeHost) {
+        cudaGetLastError();
+        return fail(SJCS_ERR_INVALID, "the step's particle buffer must be pinned host memory (sjcs_host_alloc)");
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    sjcs_step* st = new (std::nothrow) sjcs_step();
+    if (!st) return fail(SJCS_ERR_NOMEM, "out of host memory");
+    st->magic = kStepMagic;
+    st->ctx = ctx;
+    st->q = q;
+    cudaEventCreate(&st->ev_pre);
+    cudaEventCreate(&st->ev0);
+    cudaEventCreate(&st->ev1);
+    cudaEvent_t join1 = nullptr, join2 = nullptr;
+    cudaEventCreateWithFlags(&join1, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&join2, cudaEventDisableTiming);
+    sjcs_index* idx = new_index(ctx);
+    idx->kind = o.kind;
+    idx->n = n;
+    cudaError_t e = cudaStreamBeginCapture(ctx->s_build, cudaStreamCaptureModeRelaxed);
+    if (e != cudaSuccess) {
+        rc = fail(SJCS_ERR_CUDA, "stream capture could not start: %s", cudaGetErrorString(e));
+    } else {
+        rc = capture_step_body(ctx, q, host_xyz, n, o, idx, join1, join2);
+        cudaGraph_t g = nullptr;
+        e = cudaStreamEndCapture(ctx->s_build, &g);
+        if (!rc && e != cudaSuccess) rc = fail(SJCS_ERR_CUDA, "stream capture failed: %s", cudaGetErrorString(e));
+        st->graph = g;
+        if (!rc) {
+            e = cudaGraphInstantiate(&st->exec, g, 0);
+            if (e != cudaSuccess) rc = fail(SJCS_ERR_CUDA, "graph instantiation failed: %s", cudaGetErrorString(e));
+            size_t nn = 0;
+            if (!rc && cudaGraphGetNodes(g, nullptr, &nn) == cudaSuccess && nn) {
+                std::vector<cudaGraphNode_t> nodes(nn);
+                if (cudaGraphGetNodes(g, nodes.data(), &nn) == cudaSuccess)
+                    for (cudaGraphNode_t nd : nodes) {
+                        cudaGraphNodeType t;
+                        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) ++st->kernels;
+                    }
+            }
+        }
+    }
+    cudaGetLastError();
+    // The index object only described the captured buffers; its memory
+    // belongs to the graph.
+    idx->pts = nullptr;
+    idx->cell_start = nullptr;
+    idx->leaves = nullptr;
+    idx->root = nullptr;
+    free_index(idx);
+    cudaEventDestroy(join1);
+    cudaEventDestroy(join2);
+    if (rc) {
+        if (st->exec) cudaGraphExecDestroy(st->exec);
+        if (st->graph) cudaGraphDestroy(st->graph);
+        cudaEventDestroy(st->ev_pre);
+        cudaEventDestroy(st->ev0);
+        cudaEventDestroy(st->ev1);
+        st->magic = 0;
+        delete st;
+        return rc;
+    }
+    *out = st;
+    return SJCS_OK;
+}
+
+int sjcs_step_launch(sjcs_ctx* ctx, sjcs_step* st) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_step(st) || st->ctx != ctx) return fail(SJCS_ERR_STATE, "step does not belong to this context");
+    if (!valid_query(st->q)) return fail(SJCS_ERR_STATE, "the step's query was destroyed");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    // after everything queued so far on both streams (halo preparation,
+    // earlier counts and read-backs of the query)
+    SJCS_CUDA_TRY(cudaEventRecord(st->ev_pre, ctx->s_count));
+    SJCS_CUDA_TRY(cudaStreamWaitEvent(ctx->s_build, st->ev_pre, 0));
+    SJCS_CUDA_TRY(cudaEventRecord(st->ev0, ctx->s_build));
+    SJCS_CUDA_TRY(cudaGraphLaunch(st->exec, ctx->s_build));
+    for (size_t k = 0; k < st->kernels; ++k) note_launch();
+    SJCS_CUDA_TRY(cudaEventRecord(st->ev1, ctx->s_build));
+    SJCS_CUDA_TRY(cudaStreamWaitEvent(ctx->s_count, st->ev1, 0));
+    SJCS_CUDA_TRY(cudaEventRecord(st->q->ev_last, ctx->s_count));
+    st->launched = true;
+    return SJCS_OK;
+}
+
+int sjcs_step_wait(sjcs_step* st) {
+    if (!valid_step(st)) return fail(SJCS_ERR_STATE, "invalid step");
+    if (st->launched) SJCS_CUDA_TRY(cudaEventSynchronize(st->ev1));
+    return SJCS_OK;
+}
+
+int sjcs_step_time(sjcs_step* st, float* ms) {
+    if (!valid_step(st) || !ms) return fail(SJCS_ERR_INVALID, "invalid argument");
+    *ms = 0.0f;
+    if (!st->launched) return SJCS_OK;
+    SJCS_CUDA_TRY(cudaEventSynchronize(st->ev1));
+    SJCS_CUDA_TRY(cudaEventElapsedTime(ms, st->ev0, st->ev1));
+    return SJCS_OK;
+}
+
+int sjcs_step_destroy(sjcs_step* st) {
+    if (!valid_step(st)) return fail(SJCS_ERR_STATE, "invalid step");
+    set_device(st->ctx);
+    if (st->launched) cudaEventSynchronize(st->ev1);
+    cudaGraphExecDestroy(st->exec);
+    cudaGraphDestroy(st->graph);
+    cudaEventDestroy(st->ev_pre);
+    cudaEventDestroy(st->ev0);
+    cudaEventDestroy(st->ev1);
+    st->magic = 0;
+    delete st;
+    return SJCS_OK;
 }
 
 int sjcs_query_set_schedule(sjcs_ctx* ctx, sjcs_query* q, const sjcs_schedule* sched) {

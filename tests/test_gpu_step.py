@@ -1,0 +1,71 @@
+"""Captured file steps (copy + build + count as one CUDA graph) on the GPU.
+
+A replayed step must add exactly what the uncaptured calls add: the same
+counts for every index kind and schedule, file after file through the same
+pinned buffer, and mixed freely with ordinary count calls on the query.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+import pytest
+
+from spatialjoincountovershells_b200 import _native as nat
+
+pytestmark = pytest.mark.gpu
+
+
+def plain_counts(ctx, files, h, r2, kind, sched):
+    q = ctx.query(h, r2)
+    q.set_schedule(sched)
+    for f in files:
+        idx = ctx.build_index(f, radius_hint=20.0, kind=kind)
+        q.count(idx)
+        idx.destroy()
+    out = q.read_counts()
+    q.destroy()
+    return out
+
+
+@pytest.mark.parametrize("kind,sched", [(nat.INDEX_GRID, nat.SCHED_STATIC), (nat.INDEX_GRID, nat.SCHED_QUEUE),
+                                        (nat.INDEX_LEARNED, nat.SCHED_AUTO), (nat.INDEX_MORTON, nat.SCHED_AUTO)])
+def test_step_replays_match_uncaptured_calls(kind, sched, ctx):
+    n = 150000
+    files = [nat.gen_clustered_particles(s, n) for s in (41, 42, 43)]
+    h = nat.gen_clustered_halos(44, 3000)
+    r2 = nat.radius_table(0.01, 20, 64)
+    want = plain_counts(ctx, files, h, r2, kind, sched)
+    q = ctx.query(h, r2)
+    q.set_schedule(sched)
+    st = ctx.step(q, n, radius_hint=20.0, kind=kind)
+    before = nat.launch_counter()
+    for f in files:
+        st.buffer[:] = f
+        st.launch().wait()
+        assert st.time_ms() > 0
+    assert nat.launch_counter() - before >= 3 * 5  # the graph's kernels are counted
+    assert np.array_equal(q.read_counts(), want)
+    # an ordinary count call on the same query adds on top of the replays
+    idx = ctx.build_index(files[0], radius_hint=20.0, kind=kind)
+    q.count(idx)
+    st.buffer[:] = files[1]
+    st.launch()
+    q.count(idx)
+    got = q.read_counts()
+    single0 = plain_counts(ctx, files[:1], h, r2, kind, sched)
+    single1 = plain_counts(ctx, files[1:2], h, r2, kind, sched)
+    assert np.array_equal(got, want + 2 * single0 + single1)
+    idx.destroy()
+    st.destroy()
+    q.destroy()
+
+
+def test_step_needs_pinned_memory(ctx):
+    q = ctx.query(np.ones((4, 3), np.float32), nat.radius_table(0.1, 5, 8))
+    pageable = np.zeros((100, 3), np.float32)
+    h = ctypes.c_void_p()
+    rc = nat.lib().sjcs_step_create(ctx._h, q._h, ctypes.c_void_p(pageable.ctypes.data), 100,
+                                     ctypes.byref(nat.sjcs_index_opts()), ctypes.byref(h))
+    assert rc == 1 and b"pinned" in nat.lib().sjcs_last_error()
+    q.destroy()
