@@ -18,6 +18,12 @@
  * reference's backlog pipeline, main.c:266-350, on two CUDA streams); a
  * missing or unreadable input file is reported and the program exits with
  * status 1 where the reference dereferences a NULL buffer.
+ *
+ * Added (GPU options, all optional): --index grid|morton|learned picks the
+ * index form; --schedule auto|static|queue the count schedule; --autotune
+ * times the schedules on the first file and keeps the fastest; --graph runs
+ * every file step (copy, build, count) as a captured CUDA graph, reading the
+ * next file into a second pinned buffer while the current step runs.
  */
 #define _GNU_SOURCE
 #include <math.h>
@@ -133,6 +139,31 @@ static void die_lib(const char *what)
     exit(EXIT_FAILURE);
 }
 
+/* ---- GPU options ------------------------------------------------------------ */
+
+static int g_index_kind = SJCS_INDEX_GRID;
+static bool g_autotune = false;
+
+static void autotune_once(sjcs_ctx *ctx, sjcs_query *q, sjcs_index *idx)
+{
+    sjcs_schedule chosen;
+    float ms[16];
+    int nt = 0, i;
+    double t0;
+    if (!g_autotune)
+        return;
+    g_autotune = false;
+    t0 = now_us();
+    if (sjcs_autotune(ctx, q, idx, &chosen, ms, 16, &nt) != SJCS_OK)
+        die_lib("autotune");
+    printf("  autotune: schedule %s (piece %u, max pieces %u); trials:",
+           chosen.mode == SJCS_SCHED_QUEUE ? "queue" : "static", chosen.piece, chosen.max_pieces);
+    for (i = 0; i < nt && i < 16; i++)
+        printf(" %.2f", ms[i]);
+    printf(" ms\n");
+    print_ms(">>>> autotuning time", t0);
+}
+
 /* ---- one particle file in flight ------------------------------------------ */
 
 typedef struct Pending {
@@ -150,7 +181,7 @@ static void start_index(sjcs_ctx *ctx, const char *fname, float radius_hint, Pen
     uint64_t n = 0;
     double t0;
     memset(&opts, 0, sizeof(opts));
-    opts.kind = SJCS_INDEX_GRID;
+    opts.kind = g_index_kind;
     opts.radius_hint = radius_hint;
     t0 = now_us();
     if (sjcs_particle_file_count(fname, &n) != 0) {
@@ -181,7 +212,9 @@ static void finish_index(Pending *p, double t0)
 
 static void search_and_destroy(sjcs_ctx *ctx, sjcs_query *q, Pending *p)
 {
-    double t0 = now_us();
+    double t0;
+    autotune_once(ctx, q, p->idx);
+    t0 = now_us();
     if (sjcs_query_count(ctx, q, p->idx) != SJCS_OK)
         die_lib("shell count");
     if (sjcs_ctx_sync(ctx) != SJCS_OK)
@@ -246,6 +279,7 @@ static void with_backlog(sjcs_ctx *ctx, sjcs_query *q, char **files, int nfiles,
         print_ms(">>>> index getting time", t0);
         head = (head + 1) % cap;
         count--;
+        autotune_once(ctx, q, cur->idx);
         t0 = now_us();
         if (sjcs_query_count(ctx, q, cur->idx) != SJCS_OK)
             die_lib("shell count");
@@ -271,6 +305,91 @@ static void with_backlog(sjcs_ctx *ctx, sjcs_query *q, char **files, int nfiles,
     free(ring);
 }
 
+/* Every file step as a captured CUDA graph; two steps over two pinned
+ * buffers alternate so the next file is read while the current step runs. */
+static void report_step(sjcs_step *st, int file)
+{
+    float ms = 0.0f;
+    if (sjcs_step_time(st, &ms) != SJCS_OK)
+        die_lib("file step");
+    printf(">>>> file %d step time (copy + build + search): %.2f milli seconds\n", file, ms);
+}
+
+static void graph_steps(sjcs_ctx *ctx, sjcs_query *q, char **files, int nfiles, float radius_hint)
+{
+    sjcs_step *st[2] = {NULL, NULL};
+    float *buf[2] = {NULL, NULL};
+    uint64_t bufcap[2] = {0, 0}, stepn[2] = {0, 0};
+    int last[2] = {-1, -1};
+    sjcs_index_opts opts;
+    int i;
+    memset(&opts, 0, sizeof(opts));
+    opts.kind = g_index_kind;
+    opts.radius_hint = radius_hint;
+    puts("  -- with captured file steps (CUDA graphs)");
+    for (i = 0; i < nfiles; i++) {
+        const int b = i & 1;
+        uint64_t n = 0, got = 0;
+        double t0 = now_us();
+        if (sjcs_particle_file_count(files[i], &n) != 0) {
+            fprintf(stderr, "%s\n", sjcs_host_last_error());
+            exit(EXIT_FAILURE);
+        }
+        if (st[b] && last[b] >= 0) { /* this buffer's previous step must be done before the refill */
+            report_step(st[b], last[b]);
+            last[b] = -1;
+        }
+        if (!buf[b] || n > bufcap[b]) {
+            if (st[b])
+                sjcs_step_destroy(st[b]);
+            st[b] = NULL;
+            if (buf[b])
+                sjcs_host_free(buf[b]);
+            if (sjcs_host_alloc((n ? n : 1) * 3 * sizeof(float), (void **)&buf[b]) != SJCS_OK)
+                die_lib("pinned buffer");
+            bufcap[b] = n;
+        }
+        if (sjcs_read_particles(files[i], buf[b], n, &got) != 0) {
+            fprintf(stderr, "%s\n", sjcs_host_last_error());
+            exit(EXIT_FAILURE);
+        }
+        print_ms(">>>> particles reading time", t0);
+        printf("  # of particles = %llu\n", (unsigned long long)got);
+        if (got == 0)
+            continue; /* an empty file adds nothing */
+        if (g_autotune) { /* tune on this file with an ordinary build before capturing */
+            sjcs_index *idx = NULL;
+            if (sjcs_index_build(ctx, buf[b], got, &opts, &idx) != SJCS_OK || sjcs_index_wait(idx) != SJCS_OK)
+                die_lib("index build");
+            autotune_once(ctx, q, idx);
+            sjcs_index_destroy(idx);
+        }
+        if (st[b] && got != stepn[b]) { /* a captured step replays one particle count only */
+            sjcs_step_destroy(st[b]);
+            st[b] = NULL;
+        }
+        if (!st[b]) {
+            if (sjcs_step_create(ctx, q, buf[b], got, &opts, &st[b]) != SJCS_OK)
+                die_lib("file step capture");
+            stepn[b] = got;
+        }
+        if (sjcs_step_launch(ctx, st[b]) != SJCS_OK)
+            die_lib("file step");
+        last[b] = i;
+    }
+    for (i = 0; i < 2; i++) {
+        const int b = (nfiles + i) & 1; /* the older of the two last steps first */
+        if (st[b] && last[b] >= 0)
+            report_step(st[b], last[b]);
+    }
+    for (i = 0; i < 2; i++) {
+        if (st[i])
+            sjcs_step_destroy(st[i]);
+        if (buf[i])
+            sjcs_host_free(buf[i]);
+    }
+}
+
 int main(int argc, char *argv[])
 {
     char *outfile_name = NULL;
@@ -293,6 +412,9 @@ int main(int argc, char *argv[])
     sjcs_ctx *ctx = NULL;
     sjcs_query *q = NULL;
     double t0, t_total;
+    char *index_str = NULL, *sched_str = NULL;
+    int sched_mode = SJCS_SCHED_AUTO;
+    bool use_graph = false;
 
     /*** argument processing (main.c:492-602) ***/
     get_option_value(argc, argv, &outfile_name, OPT_STRING_PTR, "--output-file", 0);
@@ -334,6 +456,31 @@ int main(int argc, char *argv[])
     }
     get_option_value(argc, argv, &nthreads, OPT_INT, "--thread", 0);
     get_option_value(argc, argv, &nsetups, OPT_INT, "--next-setup", 0);
+    /* GPU options (not in the reference) */
+    get_option_value(argc, argv, &index_str, OPT_STRING_PTR, "--index", 0);
+    get_option_value(argc, argv, &sched_str, OPT_STRING_PTR, "--schedule", 0);
+    g_autotune = get_option_flag(argc, argv, "--autotune");
+    use_graph = get_option_flag(argc, argv, "--graph");
+    if (index_str != NULL) {
+        if (strcmp(index_str, "grid") == 0)
+            g_index_kind = SJCS_INDEX_GRID;
+        else if (strcmp(index_str, "morton") == 0)
+            g_index_kind = SJCS_INDEX_MORTON;
+        else if (strcmp(index_str, "learned") == 0)
+            g_index_kind = SJCS_INDEX_LEARNED;
+        else
+            set_error(&errflag, errmsg, "ERROR: --index must be grid, morton or learned");
+    }
+    if (sched_str != NULL) {
+        if (strcmp(sched_str, "auto") == 0)
+            sched_mode = SJCS_SCHED_AUTO;
+        else if (strcmp(sched_str, "static") == 0)
+            sched_mode = SJCS_SCHED_STATIC;
+        else if (strcmp(sched_str, "queue") == 0)
+            sched_mode = SJCS_SCHED_QUEUE;
+        else
+            set_error(&errflag, errmsg, "ERROR: --schedule must be auto, static or queue");
+    }
     if (nthreads < 1) {
         set_error(&errflag, errmsg,
                   "# of threads must be >= 1.\n"
@@ -440,6 +587,16 @@ int main(int argc, char *argv[])
     if (sjcs_query_create(ctx, nhalos ? halos[0].point : NULL, sizeof(sjcs_halo), nhalos, r2, nrads,
                           SJCS_QUERY_PERIODIC, &q) != SJCS_OK)
         die_lib("halo upload");
+    if (sched_mode != SJCS_SCHED_AUTO) {
+        sjcs_schedule sc;
+        memset(&sc, 0, sizeof(sc));
+        sc.mode = sched_mode;
+        if (sjcs_query_set_schedule(ctx, q, &sc) != SJCS_OK)
+            die_lib("schedule");
+    }
+    if (index_str || sched_str || g_autotune || use_graph)
+        printf("  GPU: index %s, schedule %s%s%s\n", index_str ? index_str : "grid", sched_str ? sched_str : "auto",
+               g_autotune ? ", autotuned" : "", use_graph ? ", captured file steps" : "");
 
     /*** execution ***/
     t_total = now_us();
@@ -447,7 +604,9 @@ int main(int argc, char *argv[])
         const float radius_hint = (float)sqrt((double)r2[nrads - 1]);
         char **files = &argv[particle_beg];
         const int nfiles = particle_end - particle_beg;
-        if (maxbacklogs == 0)
+        if (use_graph)
+            graph_steps(ctx, q, files, nfiles, radius_hint);
+        else if (maxbacklogs == 0)
             no_backlog(ctx, q, files, nfiles, radius_hint);
         else
             with_backlog(ctx, q, files, nfiles, maxbacklogs, first_nbacklogs, radius_hint);

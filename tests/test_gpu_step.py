@@ -69,3 +69,27 @@ def test_step_needs_pinned_memory(ctx):
                                      ctypes.byref(nat.sjcs_index_opts()), ctypes.byref(h))
     assert rc == 1 and b"pinned" in nat.lib().sjcs_last_error()
     q.destroy()
+
+
+DRIVER_OPTIONS = [["--index", "learned"], ["--index", "morton"], ["--schedule", "queue"], ["--autotune"],
+                  ["--graph"], ["--graph", "--index", "learned", "--autotune"]]
+
+
+@pytest.mark.parametrize("extra", DRIVER_OPTIONS, ids=lambda e: " ".join(e))
+@pytest.mark.parametrize("name", ["multi_file", "edge", "c1"])
+def test_driver_gpu_options_keep_the_reference_text(name, extra, case_dirs, manifest, tmp_path):
+    import hashlib
+    import subprocess
+
+    from golden import cases
+    from test_gpu_parity import DRIVER
+    d, spec = case_dirs[name]
+    out = tmp_path / "result.txt"
+    r = subprocess.run([str(DRIVER), *cases.cli_args(spec, str(out)), *extra], cwd=d, capture_output=True,
+                       text=True, timeout=600)
+    assert r.returncode == 0, r.stderr
+    assert hashlib.sha256(out.read_bytes()).hexdigest() == manifest[name]["sha256"]
+    if "--graph" in extra:
+        assert "step time" in r.stdout
+    if "--autotune" in extra:
+        assert "autotune: schedule" in r.stdout
