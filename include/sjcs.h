@@ -79,6 +79,7 @@ typedef struct sjcs_ctx   sjcs_ctx;   /* one GPU: streams, scratch, tuning cache
 typedef struct sjcs_index sjcs_index; /* device-resident index over one particle file */
 typedef struct sjcs_query sjcs_query; /* device-resident halos + radius table + u32 count accumulators */
 typedef struct sjcs_step  sjcs_step;  /* one particle file's step (copy, build, count) captured as a CUDA graph */
+typedef struct sjcs_server sjcs_server; /* request loop over device-resident indexes */
 
 /* Build options.  Zero-initialised options select an automatic grid for the
  * plain index (sized from n and radius_hint). */
@@ -275,6 +276,52 @@ int sjcs_step_wait(sjcs_step *st);
 int sjcs_step_time(sjcs_step *st, float *ms);
 /* Destroy after the last launch has finished; q must outlive its steps. */
 int sjcs_step_destroy(sjcs_step *st);
+
+/* ---- serving (no counterpart in the reference, which runs one batch job) ---- */
+
+typedef struct sjcs_server_opts {
+    uint32_t slots;       /* requests on the GPU at once, one CUDA stream each (0 = 4, at most 64) */
+    uint32_t pad_;
+    uint64_t mem_budget;  /* device bytes the admitted requests may hold together
+                             (0 = 80% of the device memory free when the server starts) */
+    uint32_t reserved[4]; /* must be zero */
+} sjcs_server_opts;
+
+typedef struct sjcs_request_info {
+    double queue_ms;      /* submission to admission (waiting for a slot or memory) */
+    double service_ms;    /* admission to detected completion */
+    double latency_ms;    /* submission to detected completion */
+    int    status;        /* SJCS_OK or the request's error */
+} sjcs_request_info;
+
+typedef struct sjcs_server_info {
+    uint64_t submitted, completed, queued;
+    uint32_t inflight, max_inflight, slots, pad_;
+    uint64_t budget_bytes, in_use_bytes, peak_bytes;
+} sjcs_server_info;
+
+/* Start a request loop over the given indexes (built in ctx, kept resident by
+ * the caller until the server is destroyed; each request's counts are summed
+ * over all of them, as the driver sums particle files).  A dispatcher thread
+ * admits requests first come first served whenever a slot is free and the
+ * request's device memory fits in the budget left by the running ones; each
+ * admitted request runs on its own stream, so requests overlap on the GPU. */
+int sjcs_server_create(sjcs_ctx *ctx, sjcs_index *const *indexes, int nindexes,
+                       const sjcs_server_opts *opts, sjcs_server **out);
+/* Queue one request: nhalos halo centres (host memory, `stride_bytes` apart),
+ * a squared-radius table and query flags as for sjcs_query_create.  When it
+ * completes, out_counts (host, uint32 [nhalos][nrads], pinned or not) holds
+ * its counts.  Both buffers must stay valid until sjcs_server_wait returns.
+ * Returns at once with a ticket; SJCS_ERR_NOMEM if the request alone needs
+ * more device memory than the budget. */
+int sjcs_server_submit(sjcs_server *srv, const float *halo_xyz, size_t stride_bytes, uint64_t nhalos,
+                       const float *r2, int nrads, int flags, uint32_t *out_counts, uint64_t *ticket);
+/* Block until the ticket's request has completed; info (may be NULL) gets its
+ * timing.  Returns the request's status.  A ticket can be waited for once. */
+int sjcs_server_wait(sjcs_server *srv, uint64_t ticket, sjcs_request_info *info);
+int sjcs_server_stats(sjcs_server *srv, sjcs_server_info *out);
+/* Finish every submitted request, then stop (before its indexes and ctx go). */
+int sjcs_server_destroy(sjcs_server *srv);
 
 /* ---- schedules and autotuning (no counterpart in the reference, whose
  * threads take halos in chunks of 100 from a shared counter,

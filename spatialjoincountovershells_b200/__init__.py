@@ -30,6 +30,7 @@ from ._native import (  # noqa: F401
     Context,
     Index,
     Query,
+    Server,
     SjcsError,
     gen_clustered_halos,
     gen_clustered_particles,

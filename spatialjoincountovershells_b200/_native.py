@@ -56,6 +56,23 @@ class sjcs_schedule(_c.Structure):
     _fields_ = [("mode", _c.c_int), ("piece", _c.c_uint32), ("max_pieces", _c.c_uint32), ("single", _c.c_uint32)]
 
 
+class sjcs_server_opts(_c.Structure):
+    _fields_ = [("slots", _c.c_uint32), ("pad_", _c.c_uint32), ("mem_budget", _c.c_uint64),
+                ("reserved", _c.c_uint32 * 4)]
+
+
+class sjcs_request_info(_c.Structure):
+    _fields_ = [("queue_ms", _c.c_double), ("service_ms", _c.c_double), ("latency_ms", _c.c_double),
+                ("status", _c.c_int)]
+
+
+class sjcs_server_info(_c.Structure):
+    _fields_ = [("submitted", _c.c_uint64), ("completed", _c.c_uint64), ("queued", _c.c_uint64),
+                ("inflight", _c.c_uint32), ("max_inflight", _c.c_uint32), ("slots", _c.c_uint32),
+                ("pad_", _c.c_uint32), ("budget_bytes", _c.c_uint64), ("in_use_bytes", _c.c_uint64),
+                ("peak_bytes", _c.c_uint64)]
+
+
 class sjcs_timing(_c.Structure):
     _fields_ = [("h2d_ms", _c.c_float), ("build_ms", _c.c_float), ("count_ms", _c.c_float),
                 ("d2h_ms", _c.c_float), ("count_calls", _c.c_uint32)]
@@ -91,6 +108,12 @@ _SIGS = {
     "sjcs_step_wait": (_c.c_int, [_vp]),
     "sjcs_step_time": (_c.c_int, [_vp, _c.POINTER(_c.c_float)]),
     "sjcs_step_destroy": (_c.c_int, [_vp]),
+    "sjcs_server_create": (_c.c_int, [_vp, _c.POINTER(_vp), _c.c_int, _c.POINTER(sjcs_server_opts), _pp]),
+    "sjcs_server_submit": (_c.c_int, [_vp, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _vp,
+                                      _c.POINTER(_u64)]),
+    "sjcs_server_wait": (_c.c_int, [_vp, _u64, _c.POINTER(sjcs_request_info)]),
+    "sjcs_server_stats": (_c.c_int, [_vp, _c.POINTER(sjcs_server_info)]),
+    "sjcs_server_destroy": (_c.c_int, [_vp]),
     "sjcs_query_set_schedule": (_c.c_int, [_vp, _vp, _c.POINTER(sjcs_schedule)]),
     "sjcs_query_get_schedule": (_c.c_int, [_vp, _c.POINTER(sjcs_schedule)]),
     "sjcs_autotune": (_c.c_int, [_vp, _vp, _vp, _c.POINTER(sjcs_schedule), _c.POINTER(_c.c_float), _c.c_int,
@@ -497,6 +520,65 @@ class Query:
                 lib().sjcs_query_destroy(self._h)
         except Exception:
             pass
+
+
+class Server:
+    """Request loop over device-resident indexes (sjcs_server_*)."""
+
+    def __init__(self, ctx: "Context", indexes, slots: int = 0, mem_budget: int = 0):
+        self.ctx = ctx
+        self._indexes = list(indexes)
+        arr = (_vp * max(1, len(self._indexes)))(*[i._h for i in self._indexes])
+        o = sjcs_server_opts()
+        o.slots = slots
+        o.mem_budget = mem_budget
+        self._h = _vp()
+        _check(lib().sjcs_server_create(ctx._h, arr, len(self._indexes), _c.byref(o), _c.byref(self._h)))
+        self._live = {}
+
+    def submit(self, halos, r2, periodic: bool = True, out: np.ndarray | None = None) -> int:
+        """Queue a request; returns its ticket.  halos: (n,3) float32 or HALO_DTYPE array."""
+        r2 = np.ascontiguousarray(r2, dtype=np.float32)
+        if isinstance(halos, np.ndarray) and halos.dtype == HALO_DTYPE:
+            arr = np.ascontiguousarray(halos)
+            base, stride = arr.ctypes.data + HALO_DTYPE.fields["point"][1], 24
+        else:
+            arr = _as_f32_xyz(halos)
+            base, stride = arr.ctypes.data, 12
+        n = arr.shape[0]
+        if out is None:
+            out = np.empty((n, len(r2)), np.uint32)
+        t = _u64()
+        _check(lib().sjcs_server_submit(self._h, _vp(base if n else 0), stride, n, _vp(r2.ctypes.data), len(r2),
+                                        QUERY_PERIODIC if periodic else QUERY_NONPERIODIC,
+                                        _vp(out.ctypes.data if n else 0), _c.byref(t)))
+        self._live[t.value] = (arr, r2, out)
+        return t.value
+
+    def wait(self, ticket: int):
+        """(counts uint32 [n, nrads], info dict) of a submitted request."""
+        info = sjcs_request_info()
+        rc = lib().sjcs_server_wait(self._h, ticket, _c.byref(info))
+        _, _, out = self._live.pop(ticket)
+        _check(rc)
+        return out, {f: getattr(info, f) for f, _ in sjcs_request_info._fields_}
+
+    def stats(self) -> dict:
+        st = sjcs_server_info()
+        _check(lib().sjcs_server_stats(self._h, _c.byref(st)))
+        return {f: getattr(st, f) for f, _ in sjcs_server_info._fields_ if f != "pad_"}
+
+    def close(self) -> None:
+        if self._h:
+            _check(lib().sjcs_server_destroy(self._h))
+            self._h = None
+            self._live.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
 
 
 def _sched_dict(sc) -> dict:

@@ -128,10 +128,10 @@ void build_shell_lut(const float* r2, int nrads, std::vector<uint32_t>* lut, uin
     *shift_out = shift;
 }
 
+}  // namespace
+
 int query_prepare(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride, uint64_t nhalos, const float* r2,
-                  int nrads, int flags, sjcs_query* q, StreamScratch* keep) {
-    (void)keep;
-    cudaStream_t s = ctx->s_count;
+                  int nrads, int flags, sjcs_query* q, cudaStream_t s) {
     q->nhalos = nhalos;
     q->nrads = nrads;
     q->flags = flags;
@@ -165,6 +165,8 @@ int query_prepare(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride, uint64_
     SJCS_CUDA_TRY(cudaMallocAsync(&q->halos, (nhalos ? nhalos : 1) * sizeof(float4), s));
     return sort_halos(ctx, d_halo_xyz, stride, nhalos, q->halos, s);
 }
+
+namespace {
 
 int check_query_args(sjcs_ctx* ctx, const float* halo_xyz, size_t stride, uint64_t nhalos, const float* r2,
                      int nrads, int flags, sjcs_query** out) {
@@ -340,6 +342,8 @@ std::string shape_key(const sjcs_query* q, const sjcs_index* idx) {
     return buf;
 }
 
+}  // namespace
+
 Schedule resolve(const sjcs_schedule& in) {
     Schedule sc{};
     sc.mode = in.mode == SJCS_SCHED_QUEUE ? SJCS_SCHED_QUEUE : SJCS_SCHED_STATIC;
@@ -359,6 +363,8 @@ Schedule schedule_for(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx)
     }
     return resolve(sc);
 }
+
+namespace {
 
 }  // namespace
 }  // namespace sjcs
@@ -648,7 +654,7 @@ int sjcs_query_create(sjcs_ctx* ctx, const float* halo_xyz, size_t stride_bytes,
             return fail(SJCS_ERR_CUDA, "halo upload failed: %s", cudaGetErrorString(e));
         }
     }
-    rc = query_prepare(ctx, d_raw, stride_bytes, nhalos, r2, nrads, flags, q, &scr);
+    rc = query_prepare(ctx, d_raw, stride_bytes, nhalos, r2, nrads, flags, q, ctx->s_count);
     if (rc) {
         free_query(q);
         return rc;
@@ -667,7 +673,7 @@ int sjcs_query_create_device(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stri
     std::lock_guard<std::mutex> lk(ctx->mu);
     sjcs_query* q = new_query(ctx);
     if (!q) return fail(SJCS_ERR_NOMEM, "out of host memory");
-    rc = query_prepare(ctx, d_halo_xyz, stride_bytes, nhalos, r2, nrads, flags, q, nullptr);
+    rc = query_prepare(ctx, d_halo_xyz, stride_bytes, nhalos, r2, nrads, flags, q, ctx->s_count);
     if (rc) {
         free_query(q);
         return rc;

@@ -193,6 +193,14 @@ int build_morton_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, int level,
 // morton_count.cu
 int launch_morton_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s);
 
+// sjcs_abi.cu: query preparation on stream s (radius table, shell lookup,
+// zeroed accumulators, Morton-sorted halos) and schedule resolution
+int query_prepare(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride, uint64_t nhalos, const float* r2,
+                  int nrads, int flags, sjcs_query* q, cudaStream_t s);
+struct Schedule;
+Schedule schedule_for(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx);
+Schedule resolve(const sjcs_schedule& in);
+
 // query_prep.cu
 int sort_halos(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride_bytes, uint64_t nhalos,
                float4* out, cudaStream_t s);
