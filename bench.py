@@ -352,7 +352,45 @@ def run_ours(args, w, dist, rank, world, local):
         bt.append(idx.timing()["build_ms"])
         idx.destroy()
     qt = q.timing()
+    q.wait()
+    grid_counts = device_counts(q).clone() if not args.no_forms else None
     q.destroy()
+
+    # the other index forms on the same workload (resident leg): the learned
+    # index and the plain Morton table, with their counts compared on the device
+    forms = None
+    if not args.no_forms:
+        forms = {}
+        for name, kind in (("learned", nat.INDEX_LEARNED), ("morton", nat.INDEX_MORTON)):
+            def fstep(kind=kind):
+                qq = ctx.query(halos_d, r2)
+                for f in range(nf):
+                    ix = ctx.build_index(parts_d[f], radius_hint=R, kind=kind)
+                    qq.count(ix)
+                    ix.destroy()
+                return qq
+            fms, flaunch, fcount, _ = time_steps(ctx, fstep, K, W, dist, local)
+            qq = ctx.query(halos_d, r2)
+            fb, info = [], None
+            for f in range(nf):
+                ix = ctx.build_index(parts_d[f], radius_hint=R, kind=kind)
+                qq.count(ix)
+                ix.wait()
+                fb.append(ix.timing()["build_ms"])
+                if kind == nat.INDEX_LEARNED and f == 0:
+                    info = ix.learned_info()
+                ix.destroy()
+            qq.wait()
+            same = bool(torch.equal(device_counts(qq), grid_counts))
+            qq.destroy()
+            forms[name] = {"value": round(nh * nf * world / (fms / 1e3), 1), "ms_per_step": round(fms, 3),
+                           "build_s_per_file": round(statistics.mean(fb) / 1e3, 5),
+                           "count_ms_per_file": round(fcount, 3) if fcount else None,
+                           "counts_identical_to_grid": same, "gpu_launches": flaunch}
+            if info:
+                forms[name]["model"] = {"leaves": info["leaves"], "max_err": info["max_err"],
+                                        "mean_err": round(info["mean_err"], 1), "level": info["level"]}
+        del grid_counts
     # correctness spot-check of the timed path on a halo sample (oracle, file 0)
     check = None
     if rank == 0 and not args.no_check and not args.no_e2e:
@@ -389,7 +427,7 @@ def run_ours(args, w, dist, rank, world, local):
         "dtype": "f32", "data": "synthetic: reference generator streams (MT19937 seeds 1 and 2)",
         "config": {"workload": workload_name(w), "index": "grid (radix-sorted cell table)",
                    "parallelism": "replicas" if world > 1 else "single",
-                   "l2": "inputs larger than L2 (3 x 1.2 GB particle arrays per step)"},
+                   "l2": f"inputs larger than L2 ({nf} x {n * 12 / 1e9:.2f} GB particle arrays per step)"},
         "build_s_per_file": round(statistics.mean(bt) / 1e3, 5),
         "search_halos_per_s": round(nh * nf / (qt["count_ms"] / 1e3), 1) if qt["count_ms"] else None,
         "e2e": None if args.no_e2e else {
@@ -403,9 +441,416 @@ def run_ours(args, w, dist, rank, world, local):
         "gpu_launches": int(launches),
         "gpu_launches_e2e": int(launches_e2e),
         "parity_spot_check": check,
+        "forms": forms,
     }
     ctx.close()
     return line
+
+
+# ---------------------------------------------------------------------------
+# clustered workloads: persistent schedule (config C3), index forms (C4),
+# serving (C5).  Each prints its own JSON line; the default line is C2.
+# ---------------------------------------------------------------------------
+
+CLUSTERED = dict(workload="clustered", nfiles=3, nparticles=100_000_000, nhalos=10_000_000,
+                 radius=(0.01, 20.0, 64), pseed=31, hseed=32)
+FORMS = dict(CLUSTERED, workload="learned", radius=(0.001, 5.0, 40))
+SERVING = dict(workload="serving", nfiles=3, nparticles=100_000_000, nrequests=2000, size=(1e2, 1e6),
+               nrads=(8, 64), rmax=(1.0, 10.0), arrival_seed=51, pseed=31, hseed=32)
+
+
+def clustered_name(w) -> str:
+    mn, mx, nr = w["radius"]
+    return (f"clustered {w['nfiles']} files x {w['nparticles']:.0e} particles (60% in 1e4 Gaussian clumps, "
+            f"sigma log-uniform [2,20], lognormal(0,1.5) weights; seeds {w['pseed']}+file, clumps 31), "
+            f"{w['nhalos']:.0e} halos (70% at clump centres, jitter 1; seed {w['hseed']}), "
+            f"--radius {mn}:{mx}:{nr} periodic")
+
+
+class _DeviceU32:
+    """A device u32 array seen by torch (zero-copy, via __cuda_array_interface__)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<i4", "data": (ptr, False), "version": 3}
+
+
+def device_counts(q):
+    import torch
+    return torch.as_tensor(_DeviceU32(q.device_counts_ptr, q.nhalos * q.nrads), device="cuda")
+
+
+def clustered_inputs(w):
+    """Pinned host particles (all files) and halos of a clustered workload."""
+    import numpy as np
+    import torch
+
+    from spatialjoincountovershells_b200 import _native as nat
+    n, nf = w["nparticles"], w["nfiles"]
+    parts_h = torch.empty((nf * n, 3), dtype=torch.float32, pin_memory=True)
+    for f in range(nf):
+        parts_h[f * n:(f + 1) * n] = torch.from_numpy(nat.gen_clustered_particles(w["pseed"] + f, n))
+    halos = nat.gen_clustered_halos(w["hseed"], w["nhalos"])
+    halos_h = torch.empty((w["nhalos"] * 24,), dtype=torch.uint8, pin_memory=True)
+    hnp = halos_h.numpy().view(nat.HALO_DTYPE)
+    hnp[:] = halos
+    return parts_h, halos_h, hnp, np.ascontiguousarray(halos["point"])
+
+
+def time_steps(ctx, step, K, W, dist, local):
+    """W untimed then K timed steps (one job each) on the context's streams."""
+    import torch
+
+    from spatialjoincountovershells_b200 import _native as nat
+    s_build = torch.cuda.ExternalStream(ctx.stream(0))
+    s_count = torch.cuda.ExternalStream(ctx.stream(1))
+    for _ in range(W):
+        q = step()
+        ctx.sync()
+        q.destroy()
+    dist_barrier(dist, local)
+    torch.cuda.synchronize()
+    ctx.sync()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    l0 = nat.launch_counter()
+    qs = []
+    with ClockSampler(local) as clk:
+        e0.record(s_count)
+        s_build.wait_event(e0)
+        for _ in range(K):
+            q = step()
+            q.wait()
+            qs.append(q)
+        e1.record(s_count)
+        e1.synchronize()
+    launches = nat.launch_counter() - l0
+    ctx.sync()
+    dist_barrier(dist, local)
+    ms = dist_max(dist, e0.elapsed_time(e1) / K, local)
+    cnt, calls = 0.0, 0
+    for q in qs:
+        t = q.timing()
+        cnt += t["count_ms"]
+        calls += t["count_calls"]
+        q.destroy()
+    return ms, int(launches), (cnt / calls if calls else None), clk.summary()
+
+
+def reference_sample_clustered(w, particles_file0, halos_sample, tmp: pathlib.Path):
+    from spatialjoincountovershells_b200 import _native as nat
+    pf, hf = tmp / "part0.dat", tmp / "halo_sample.list"
+    nat.write_particle_file(pf, particles_file0)
+    nat.write_halo_file(hf, halos_sample)
+    return pf, hf
+
+
+def clustered_cpu_baseline(w, particles_file0, halos, nhs):
+    from oracle import oracle
+    if not oracle.ref_available():
+        return None
+    with tempfile.TemporaryDirectory(prefix="sjcs_refcl_") as td:
+        pf, hf = reference_sample_clustered(w, particles_file0, halos[:nhs], pathlib.Path(td))
+        T = ref_threads()
+        b, s_ = run_reference_once(w, pf, hf, T)
+    v = w["nhalos"] * w["nfiles"] / (w["nfiles"] * (b + s_ * w["nhalos"] / nhs))
+    return {"value": round(v, 1), "unit": UNIT, "cores": T, "kind": "reference",
+            "sample": f"astr_rcount --thread {T} --next-setup {T} on 1 clustered file of {w['nparticles']:.0e} "
+                      f"particles x the first {nhs} halos; build {b:.3f} s, search {s_:.3f} s; extrapolated to "
+                      f"{w['nfiles']} files x {w['nhalos']:.0e} halos"}
+
+
+def run_clustered(args, w, dist, rank, world, local):
+    """C3: clustered uneven load; autotuned persistent schedule; captured file steps."""
+    import numpy as np
+    import torch
+
+    from spatialjoincountovershells_b200 import _native as nat
+    torch.cuda.set_device(local)
+    n, nf, nh = w["nparticles"], w["nfiles"], w["nhalos"]
+    mn, mx, nr = w["radius"]
+    r2 = nat.radius_table(mn, mx, nr)
+    R = math.sqrt(float(r2[-1]))
+    parts_h, halos_h, hnp, hpts = clustered_inputs(w)
+    pnp = parts_h.numpy()
+    out_np = np.empty((nh, nr), np.uint64)
+    ctx = nat.Context(local)
+    ctx.reserve(4 * (n * 16 + int(1.6 * n + 4096) * 4) + n * 44 + 4 * nh * (16 + 4 * nr + 64) + (2 << 30))
+    parts_d = [torch.from_numpy(pnp[f * n:(f + 1) * n]).cuda() for f in range(nf)]
+    halos_d = torch.from_numpy(hpts).cuda()
+    torch.cuda.synchronize()
+
+    # autotune on file 0 (the choice is cached in the context for this shape)
+    idx0 = ctx.build_index(parts_d[0], radius_hint=R)
+    qt = ctx.query(halos_d, r2)
+    tune = ctx.autotune(qt, idx0)
+    qt.destroy()
+    idx0.destroy()
+
+    def step_resident(mode):
+        def step():
+            q = ctx.query(halos_d, r2)
+            q.set_schedule(mode)
+            for f in range(nf):
+                idx = ctx.build_index(parts_d[f], radius_hint=R)
+                q.count(idx)
+                idx.destroy()
+            return q
+        return step
+
+    def step_e2e():
+        q = ctx.query(hnp, r2)
+        for f in range(nf):
+            idx = ctx.build_index(pnp[f * n:(f + 1) * n], radius_hint=R)
+            q.count(idx)
+            idx.destroy()
+        q.read_counts(out=out_np)
+        return q
+
+    K, W = args.steps, args.warmup
+    ms, launches, count_ms, clocks = time_steps(ctx, step_resident(nat.SCHED_AUTO), K, W, dist, local)
+    ms_static, _, count_static, _ = time_steps(ctx, step_resident(nat.SCHED_STATIC), K, W, dist, local)
+    ms_e2e, launches_e2e, _, clocks_e2e = time_steps(ctx, step_e2e, K, W, dist, local)
+
+    # captured file steps (graph replays of copy + build + count) against the
+    # same query, after W warm-up replays
+    q = ctx.query(halos_d, r2)
+    st = ctx.step(q, n, radius_hint=R)
+    gms = []
+    for k in range(W + K):
+        st.buffer[:] = pnp[(k % nf) * n:((k % nf) + 1) * n]
+        st.launch().wait()
+        if k >= W:
+            gms.append(st.time_ms())
+    st.destroy()
+    q.destroy()
+
+    check = None
+    if rank == 0 and not args.no_check:
+        from oracle import oracle
+        sample = 300
+        want = np.zeros((sample, nr), np.uint64)
+        for f in range(nf):
+            oracle.count(pnp[f * n:(f + 1) * n], hnp[:sample], r2, counts=want)
+        check = bool(np.array_equal(out_np[:sample], want))
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu = clustered_cpu_baseline(w, pnp[:n], hnp, 2000)
+    units = nh * nf * world
+    line = {
+        "metric": "halos/s (clustered uneven load, persistent schedule)", "value": round(units / (ms / 1e3), 1),
+        "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": round(ms, 3),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: project generators (clumped particles and halos, MT19937)",
+        "config": {"workload": clustered_name(w), "index": "grid", "schedule": tune["chosen"],
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "l2": f"inputs larger than L2 ({nf} x {n * 12 / 1e9:.2f} GB particle arrays per step)"},
+        "autotune_trial_ms": [round(t, 2) for t in tune["trial_ms"]],
+        "count_ms_per_file": round(count_ms, 2) if count_ms else None,
+        "static_schedule": {"value": round(units / (ms_static / 1e3), 1), "ms_per_step": round(ms_static, 3),
+                            "count_ms_per_file": round(count_static, 2) if count_static else None},
+        "captured_step_ms_per_file": round(statistics.mean(gms), 3),
+        "e2e": {"value": round(units / (ms_e2e / 1e3), 1), "unit": UNIT, "ms_per_step": round(ms_e2e, 3),
+                "h2d_bytes_per_step": int(nf * n * 12 + (nh - 1) * 24 + 12), "d2h_bytes_per_step": int(nh * nr * 8)},
+        "roofline": None, "cpu_baseline": cpu, "clocks": clocks, "clocks_e2e": clocks_e2e,
+        "gpu_launches": launches, "gpu_launches_e2e": launches_e2e, "parity_spot_check": check,
+    }
+    ctx.close()
+    return line
+
+
+def run_forms(args, w, dist, rank, world, local):
+    """C4: learned index vs plain forms on the clustered data, counts compared on the device."""
+    import torch
+
+    from spatialjoincountovershells_b200 import _native as nat
+    torch.cuda.set_device(local)
+    n, nf, nh = w["nparticles"], w["nfiles"], w["nhalos"]
+    mn, mx, nr = w["radius"]
+    r2 = nat.radius_table(mn, mx, nr)
+    R = math.sqrt(float(r2[-1]))
+    parts_h, halos_h, hnp, hpts = clustered_inputs(w)
+    pnp = parts_h.numpy()
+    ctx = nat.Context(local)
+    ctx.reserve(4 * (n * 16 + int(1.6 * n + 4096) * 4) + n * 60 + 4 * nh * (16 + 4 * nr + 64) + (2 << 30))
+    parts_d = [torch.from_numpy(pnp[f * n:(f + 1) * n]).cuda() for f in range(nf)]
+    halos_d = torch.from_numpy(hpts).cuda()
+    torch.cuda.synchronize()
+    idx0 = ctx.build_index(parts_d[0], radius_hint=R)
+    qt = ctx.query(halos_d, r2)
+    tune = ctx.autotune(qt, idx0)
+    qt.destroy()
+    idx0.destroy()
+
+    forms = [("grid", nat.INDEX_GRID, nat.SCHED_AUTO), ("grid-static", nat.INDEX_GRID, nat.SCHED_STATIC),
+             ("morton", nat.INDEX_MORTON, nat.SCHED_AUTO), ("learned", nat.INDEX_LEARNED, nat.SCHED_AUTO)]
+    K, W = args.steps, args.warmup
+    res, ref_counts, info = {}, None, None
+    for name, kind, mode in forms:
+        def step(kind=kind, mode=mode):
+            q = ctx.query(halos_d, r2)
+            q.set_schedule(mode)
+            for f in range(nf):
+                idx = ctx.build_index(parts_d[f], radius_hint=R, kind=kind)
+                q.count(idx)
+                idx.destroy()
+            return q
+        ms, launches, count_ms, clocks = time_steps(ctx, step, K, W, dist, local)
+        # one more pass for the build split and the counts
+        q = ctx.query(halos_d, r2)
+        q.set_schedule(mode)
+        bts = []
+        for f in range(nf):
+            idx = ctx.build_index(parts_d[f], radius_hint=R, kind=kind)
+            q.count(idx)
+            idx.wait()
+            bts.append(idx.timing()["build_ms"])
+            if kind == nat.INDEX_LEARNED and f == 0:
+                info = idx.learned_info()
+            idx.destroy()
+        q.wait()
+        c = device_counts(q)
+        if ref_counts is None:
+            ref_counts = c.clone()
+            same = True
+        else:
+            same = bool(torch.equal(c, ref_counts))
+        q.destroy()
+        res[name] = {"value": round(nh * nf * world / (ms / 1e3), 1), "ms_per_step": round(ms, 3),
+                     "build_s_per_file": round(statistics.mean(bts) / 1e3, 5),
+                     "count_ms_per_file": round(count_ms, 3) if count_ms else None,
+                     "counts_identical_to_grid": same, "gpu_launches": launches, "clocks": clocks}
+    del ref_counts
+    line = {
+        "metric": METRIC, "value": res["learned"]["value"], "unit": UNIT, "n_gpus": world, "steps": K,
+        "warmup": W, "ms_per_step": res["learned"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: project generators (clumped particles and halos, MT19937)",
+        "config": {"workload": clustered_name(w), "index": "learned (63-bit Morton, 2-level PLM, 4096 leaves)",
+                   "parallelism": "replicas" if world > 1 else "single", "grid_schedule": tune["chosen"]},
+        "plain_value": res["grid"]["value"], "forms": res,
+        "learned_info": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in (info or {}).items()},
+        "gpu_launches": res["learned"]["gpu_launches"], "clocks": res["learned"]["clocks"],
+    }
+    ctx.close()
+    return line
+
+
+def run_serving(args, w, dist, rank, world, local):
+    """C5: request loop over resident clustered indexes, Poisson arrivals, p50/p99."""
+    import numpy as np
+    import torch
+
+    from spatialjoincountovershells_b200 import _native as nat
+    torch.cuda.set_device(local)
+    n, nf = w["nparticles"], w["nfiles"]
+    rng = np.random.default_rng(w["arrival_seed"])
+    nreq = w["nrequests"]
+    lo, hi = w["size"]
+    sizes = np.round(np.exp(rng.uniform(math.log(lo), math.log(hi), nreq))).astype(np.int64)
+    nrads = rng.integers(w["nrads"][0], w["nrads"][1] + 1, nreq)
+    rmax = rng.uniform(w["rmax"][0], w["rmax"][1], nreq)
+    tables = [nat.radius_table(0.001, float(rm), int(k)) for rm, k in zip(rmax, nrads)]
+    halos = [np.ascontiguousarray(nat.gen_clustered_halos(w["hseed"] * 1000 + i, int(m))["point"])
+             for i, m in enumerate(sizes)]
+    ctx = nat.Context(local)
+    idx = []
+    for f in range(nf):
+        p = torch.from_numpy(nat.gen_clustered_particles(w["pseed"] + f, n)).cuda()
+        idx.append(ctx.build_index(p, radius_hint=w["rmax"][1]))
+        idx[-1].wait()
+        del p
+    torch.cuda.empty_cache()
+    ctx.trim()
+
+    import hashlib
+    import queue as pyqueue
+    import threading as th
+    # pinned result buffers, recycled: the counts go straight from the device
+    maxcnt = int(max(int(sizes[i]) * int(nrads[i]) for i in range(nreq)))
+    pool = pyqueue.Queue()
+    pinned = [nat.PinnedBuffer((maxcnt,), np.uint32) for _ in range(24)]
+    for b in pinned:
+        pool.put(b)
+
+    def digest(a):
+        return hashlib.blake2b(a.tobytes(), digest_size=16).hexdigest()
+
+    def run_stream(order, rate, slots):
+        """Submit `order` at Poisson times (rate per second); wait in order; latencies."""
+        srv = nat.Server(ctx, idx, slots=slots)
+        arr = np.cumsum(np.random.default_rng(w["arrival_seed"] + 1).exponential(1.0 / rate, len(order)))
+        tickets, lat, done_q = [], [], []
+        lock = th.Lock()
+
+        def waiter():
+            k = 0
+            while k < len(order):
+                with lock:
+                    t = tickets[k] if k < len(tickets) else None
+                if t is None:
+                    time.sleep(0.0002)
+                    continue
+                tk, buf, m = t
+                out, info = srv.wait(tk)
+                lat.append(info["latency_ms"])
+                done_q.append((order[k], digest(out), info["queue_ms"]))
+                pool.put(buf)
+                k += 1
+        wt = th.Thread(target=waiter)
+        wt.start()
+        t0 = time.perf_counter()
+        for k, i in enumerate(order):
+            d = t0 + arr[k] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            buf = pool.get()
+            m = int(sizes[i]) * int(nrads[i])
+            out = buf.array[:m].reshape(int(sizes[i]), int(nrads[i]))
+            t = srv.submit(halos[i], tables[i], out=out)
+            with lock:
+                tickets.append((t, buf, m))
+        wt.join()
+        makespan = time.perf_counter() - t0
+        st = srv.stats()
+        srv.close()
+        return lat, makespan, st, done_q
+
+    halo_files = int(sizes.sum()) * nf
+    # capacity: the first 200 requests submitted at once
+    cal = list(range(min(200, nreq)))
+    lat_c, span_c, _, _ = run_stream(cal, 1e9, 8)
+    cap = sum(int(sizes[i]) for i in cal) / span_c  # halos per second
+    rate = 0.7 * cap / float(sizes.mean())
+    lat, makespan, st, done = run_stream(list(range(nreq)), rate, 8)
+    lat_sorted = sorted(lat)
+    p50 = lat_sorted[len(lat) // 2]
+    p99 = lat_sorted[min(len(lat) - 1, int(math.ceil(0.99 * len(lat))) - 1)]
+    # exactness: a sample of requests again, alone (one slot, one at a time)
+    sums = {i: s for i, s, _ in done}
+    alone_ok = True
+    with nat.Server(ctx, idx, slots=1) as srv1:
+        for i in list(range(0, nreq, max(1, nreq // 20))):
+            out, _ = srv1.wait(srv1.submit(halos[i], tables[i]))
+            alone_ok &= digest(out) == sums[i]
+    for b in pinned:
+        b.free()
+    for x in idx:
+        x.destroy()
+    ctx.close()
+    return {
+        "metric": "serving: p50/p99 request latency and halos/s (Poisson arrivals, memory admission)",
+        "value": round(halo_files / makespan, 1), "unit": "halo-files/s", "n_gpus": world, "steps": 1,
+        "warmup": 1, "ms_per_step": round(makespan * 1e3, 1), "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic: project generators",
+        "config": {"workload": f"serving: {nreq} requests, sizes log-uniform [{lo:.0e},{hi:.0e}] clustered halos, "
+                               f"radius 0.001:U[{w['rmax'][0]},{w['rmax'][1]}]:U{{{w['nrads'][0]}..{w['nrads'][1]}}}, "
+                               f"Poisson arrivals at 70% of measured capacity (seed {w['arrival_seed']}), "
+                               f"{nf} resident indexes x {n:.0e} clustered particles", "slots": 8},
+        "latency_ms": {"p50": round(p50, 2), "p99": round(p99, 2), "mean": round(statistics.mean(lat), 2),
+                       "max": round(lat_sorted[-1], 2)},
+        "arrival_rate_per_s": round(rate, 2), "capacity_halos_per_s": round(cap, 1),
+        "server": st, "results_same_alone_and_in_mix": bool(alone_ok),
+        "mean_queue_ms": round(statistics.mean(q for _, _, q in done), 2),
+    }
 
 
 def cpu_baseline_leg(w, particles_file0, halos, r2):
@@ -486,6 +931,10 @@ def main():
                     help="keep only halos with z < SLAB (profiling at full halo density on fewer halos)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--no-forms", action="store_true", help="skip the learned/Morton comparison legs")
+    ap.add_argument("--workload", choices=["uniform", "clustered", "learned", "serving"], default="uniform",
+                    help="uniform: the headline line (README scale); clustered: persistent schedule and captured "
+                         "steps; learned: index forms on clustered data; serving: the request loop")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -501,6 +950,26 @@ def main():
         print(json.dumps(run_reference_arm(args, w)), flush=True)
         return
     dist, rank, world, local = dist_setup()
+    if args.workload != "uniform":
+        base = {"clustered": CLUSTERED, "learned": FORMS, "serving": SERVING}[args.workload]
+        w = dict(base)
+        if args.small:
+            w["nparticles"] //= 50
+            if "nhalos" in w:
+                w["nhalos"] //= 50
+            if "nrequests" in w:
+                w["nrequests"] //= 10
+                w["size"] = (w["size"][0], w["size"][1] / 50)
+        if args.files:
+            w["nfiles"] = args.files
+        if args.halos and "nhalos" in w:
+            w["nhalos"] = args.halos
+        run = {"clustered": run_clustered, "learned": run_forms, "serving": run_serving}[args.workload]
+        line = run(args, w, dist, rank, world, local)
+        dist_close(dist)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        return
     line = run_ours(args, w, dist, rank, world, local)
     dist_close(dist)
     if rank == 0:
