@@ -353,7 +353,7 @@ def run_ours(args, w, dist, rank, world, local):
         idx.destroy()
     qt = q.timing()
     q.wait()
-    grid_counts = device_counts(q).clone() if not args.no_forms else None
+    grid_counts = device_counts(q) if not args.no_forms else None
     q.destroy()
 
     # the other index forms on the same workload (resident leg): the learned
@@ -475,8 +475,14 @@ class _DeviceU32:
 
 
 def device_counts(q):
+    """A copy of the query's device accumulators (torch, u32 bits as int32).  The
+    copy is finished before returning: the query's memory goes back to the
+    library's pool when the query is destroyed, and torch's stream is not
+    ordered with the library's."""
     import torch
-    return torch.as_tensor(_DeviceU32(q.device_counts_ptr, q.nhalos * q.nrads), device="cuda")
+    c = torch.as_tensor(_DeviceU32(q.device_counts_ptr, q.nhalos * q.nrads), device="cuda").clone()
+    torch.cuda.synchronize()
+    return c
 
 
 def clustered_inputs(w):
@@ -709,7 +715,7 @@ def run_forms(args, w, dist, rank, world, local):
         q.wait()
         c = device_counts(q)
         if ref_counts is None:
-            ref_counts = c.clone()
+            ref_counts = c
             same = True
         else:
             same = bool(torch.equal(c, ref_counts))
