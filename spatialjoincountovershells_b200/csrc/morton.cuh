@@ -112,4 +112,52 @@ __device__ __forceinline__ uint32_t learned_rank(const LearnedRoot& rt, const Le
     return lo;
 }
 
+// N exact lower bounds at once (as learned_rank), the N bounded binary
+// searches advanced together so their probes are independent loads in flight
+// at the same time.  act[j] == false: out[j] = 0 and no memory is read.
+template <int N>
+__device__ __forceinline__ void learned_rank_n(const LearnedRoot& rt, const LearnedLeaf* __restrict__ leaves,
+                                               const uint32_t* __restrict__ wpref, const uint64_t (&q)[N],
+                                               const bool (&act)[N], uint32_t (&out)[N]) {
+    uint32_t lo[N], hi[N], qp[N];
+#pragma unroll
+    for (int j = 0; j < N; ++j) {
+        lo[j] = 0u;
+        hi[j] = 0u;
+        qp[j] = (uint32_t)(q[j] >> 33);
+        if (!act[j]) continue;
+        if (q[j] <= rt.kmin) continue;  // rank 0
+        if (q[j] > rt.kmax) {
+            lo[j] = hi[j] = rt.n;
+            continue;
+        }
+        const LearnedLeaf lf = leaves[leaf_of(rt, q[j])];
+        const uint32_t P = leaf_predict(lf, q[j]);
+        lo[j] = (P - lf.r0 > lf.err) ? P - lf.err : lf.r0;
+        const uint64_t h64 = (uint64_t)P + lf.err + 1ull;
+        hi[j] = h64 < (uint64_t)lf.r1 ? (uint32_t)h64 : lf.r1;
+    }
+    for (;;) {
+        bool any = false;
+#pragma unroll
+        for (int j = 0; j < N; ++j) any |= lo[j] < hi[j];
+        if (!any) break;
+        uint32_t v[N], mid[N];
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            mid[j] = lo[j] + ((hi[j] - lo[j]) >> 1);
+            v[j] = lo[j] < hi[j] ? __ldg(wpref + 4ull * mid[j]) : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < N; ++j) {
+            if (lo[j] < hi[j]) {
+                if (v[j] < qp[j]) lo[j] = mid[j] + 1u;
+                else hi[j] = mid[j];
+            }
+        }
+    }
+#pragma unroll
+    for (int j = 0; j < N; ++j) out[j] = lo[j];
+}
+
 }  // namespace sjcs

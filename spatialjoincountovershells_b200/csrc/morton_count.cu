@@ -51,17 +51,6 @@ struct RootRegs {
     bool table_only;  // the judge found a mismatch: the table answers
 };
 
-template <int LOOK>
-__device__ __forceinline__ uint32_t cell_rank(const MortonParams& m, const RootRegs& rr, uint32_t code) {
-    if (LOOK == LOOK_TABLE || rr.table_only) return __ldg(m.table + code);
-    LearnedRoot rt;
-    rt.kmin = rr.kmin;
-    rt.kmax = rr.kmax;
-    rt.shift = rr.shift;
-    rt.n = rr.n;
-    return learned_rank(rt, m.leaves, m.wpref, (unsigned long long)code << m.key_shift);
-}
-
 __device__ __forceinline__ int mcell_lo(const MortonParams& m, float v) { return (int)(morton_q(v) >> m.sh); }
 __device__ __forceinline__ int mcell_hi(const MortonParams& m, float v) {
     // a NaN upper bound passes every particle on that side: open to the edge
@@ -90,37 +79,58 @@ __device__ __forceinline__ void count_image_m(const CountParams& p, const Morton
     const uint32_t total = nx * ny * nz;  // <= 2^30 (L <= 10)
     const uint32_t lt = (1u << lane) - 1u;
     uint32_t npend = 0;
-    for (uint32_t cb = 0; cb < total; cb += 32u) {
-        const uint32_t k = cb + (uint32_t)lane;
-        bool keep = k < total;
-        const uint32_t t = k / nx;
-        const int xx = x0 + (int)(k - t * nx), yy = y0 + (int)(t % ny), zz = z0 + (int)(t / ny);
-        if (keep && p.prune) {
-            const float gx = cell_gap(cx, xx, m.h, m.G), gy = cell_gap(cy, yy, m.h, m.G),
-                        gz = cell_gap(cz, zz, m.h, m.G);
-            const float rem = __fadd_rn(
-                __fsub_rn(__fsub_rn(__fsub_rn(p.r2p, __fmul_rn(gx, gx)), __fmul_rn(gy, gy)), __fmul_rn(gz, gz)),
-                p.r2slack);
-            keep = rem >= 0.0f;  // no particle of this cell can be within R otherwise
+    // 64 box cells per round, two per lane: the four lookups of a lane (both
+    // ends of both cells) go out together
+    for (uint32_t cb = 0; cb < total; cb += 64u) {
+        uint32_t code[2];
+        bool keep[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const uint32_t k = cb + 32u * (uint32_t)u + (uint32_t)lane;
+            keep[u] = k < total;
+            const uint32_t t = k / nx;
+            const int xx = x0 + (int)(k - t * nx), yy = y0 + (int)(t % ny), zz = z0 + (int)(t / ny);
+            if (keep[u] && p.prune) {
+                const float gx = cell_gap(cx, xx, m.h, m.G), gy = cell_gap(cy, yy, m.h, m.G),
+                            gz = cell_gap(cz, zz, m.h, m.G);
+                const float rem = __fadd_rn(__fsub_rn(__fsub_rn(__fsub_rn(p.r2p, __fmul_rn(gx, gx)), __fmul_rn(gy, gy)),
+                                                      __fmul_rn(gz, gz)),
+                                            p.r2slack);
+                keep[u] = rem >= 0.0f;  // no particle of this cell can be within R otherwise
+            }
+            code[u] = keep[u] ? morton_cell((uint32_t)xx, (uint32_t)yy, (uint32_t)zz) : 0u;
         }
-        uint32_t s0 = 0, s1 = 0;
-        if (keep) {
-            const uint32_t code = morton_cell((uint32_t)xx, (uint32_t)yy, (uint32_t)zz);
-            s0 = cell_rank<LOOK>(m, rr, code);
-            s1 = cell_rank<LOOK>(m, rr, code + 1u);
+        uint32_t s[4];
+        if (LOOK == LOOK_TABLE || rr.table_only) {
+#pragma unroll
+            for (int j = 0; j < 4; ++j) s[j] = keep[j >> 1] ? __ldg(m.table + code[j >> 1] + (j & 1)) : 0u;
+        } else {
+            LearnedRoot rt;
+            rt.kmin = rr.kmin;
+            rt.kmax = rr.kmax;
+            rt.shift = rr.shift;
+            rt.n = rr.n;
+            const uint64_t qk[4] = {(uint64_t)code[0] << m.key_shift, (uint64_t)(code[0] + 1u) << m.key_shift,
+                                    (uint64_t)code[1] << m.key_shift, (uint64_t)(code[1] + 1u) << m.key_shift};
+            const bool act[4] = {keep[0], keep[0], keep[1], keep[1]};
+            learned_rank_n<4>(rt, m.leaves, m.wpref, qk, act, s);
         }
-        const bool ne = s1 > s0;
-        const uint32_t bal = __ballot_sync(0xffffffffu, ne);
-        if (ne) pend[npend + __popc(bal & lt)] = make_uint2(s0, s1);
-        npend += __popc(bal);
-        if (npend >= 32u) {
-            __syncwarp();
-            const uint2 r = pend[lane];
-            __syncwarp();
-            if ((uint32_t)lane < npend - 32u) pend[lane] = pend[32 + lane];
-            __syncwarp();
-            npend -= 32u;
-            run_rows<BIN, BIG>(p, im, r.x, r.y, sink, tab, lut, lane);
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const uint32_t s0 = s[2 * u], s1 = s[2 * u + 1];
+            const bool ne = keep[u] && s1 > s0;
+            const uint32_t bal = __ballot_sync(0xffffffffu, ne);
+            if (ne) pend[npend + __popc(bal & lt)] = make_uint2(s0, s1);
+            npend += __popc(bal);
+            if (npend >= 32u) {
+                __syncwarp();
+                const uint2 r = pend[lane];
+                __syncwarp();
+                if ((uint32_t)lane < npend - 32u) pend[lane] = pend[32 + lane];
+                __syncwarp();
+                npend -= 32u;
+                run_rows<BIN, BIG>(p, im, r.x, r.y, sink, tab, lut, lane);
+            }
         }
     }
     if (npend) {
