@@ -269,7 +269,8 @@ def run_ours(args, w, dist, rank, world, local):
     # grow the device pool once, so no step takes new memory from the driver:
     # K+1 queries, 4 indexes and one build's scratch
     idx_bytes = n * 16 + int(1.6 * n + 4096) * 4
-    ctx.reserve((args.steps + 1) * nh * (16 + 4 * nr + 48) + 4 * idx_bytes + n * 44 + (1 << 30))
+    if not args.no_reserve:
+        ctx.reserve((args.steps + 1) * nh * (16 + 4 * nr + 48) + 4 * idx_bytes + n * 44 + (1 << 30))
     s_build = torch.cuda.ExternalStream(ctx.stream(0))
     s_count = torch.cuda.ExternalStream(ctx.stream(1))
 
@@ -579,7 +580,8 @@ def run_clustered(args, w, dist, rank, world, local):
     pnp = parts_h.numpy()
     out_np = np.empty((nh, nr), np.uint64)
     ctx = nat.Context(local)
-    ctx.reserve(4 * (n * 16 + int(1.6 * n + 4096) * 4) + n * 44 + 4 * nh * (16 + 4 * nr + 64) + (2 << 30))
+    if not args.no_reserve:
+        ctx.reserve(4 * (n * 16 + int(1.6 * n + 4096) * 4) + n * 44 + 4 * nh * (16 + 4 * nr + 64) + (2 << 30))
     parts_d = [torch.from_numpy(pnp[f * n:(f + 1) * n]).cuda() for f in range(nf)]
     halos_d = torch.from_numpy(hpts).cuda()
     torch.cuda.synchronize()
@@ -676,7 +678,8 @@ def run_forms(args, w, dist, rank, world, local):
     parts_h, halos_h, hnp, hpts = clustered_inputs(w)
     pnp = parts_h.numpy()
     ctx = nat.Context(local)
-    ctx.reserve(4 * (n * 16 + int(1.6 * n + 4096) * 4) + n * 60 + 4 * nh * (16 + 4 * nr + 64) + (2 << 30))
+    if not args.no_reserve:
+        ctx.reserve(4 * (n * 16 + int(1.6 * n + 4096) * 4) + n * 60 + 4 * nh * (16 + 4 * nr + 64) + (2 << 30))
     parts_d = [torch.from_numpy(pnp[f * n:(f + 1) * n]).cuda() for f in range(nf)]
     halos_d = torch.from_numpy(hpts).cuda()
     torch.cuda.synchronize()
@@ -938,6 +941,9 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-check", action="store_true")
     ap.add_argument("--no-forms", action="store_true", help="skip the learned/Morton comparison legs")
+    ap.add_argument("--particles", type=int, default=None, help="override particles per file (profiling cases)")
+    ap.add_argument("--no-reserve", action="store_true",
+                    help="do not grow the device memory pool up front (profiling cases: keep the footprint small)")
     ap.add_argument("--workload", choices=["uniform", "clustered", "learned", "serving"], default="uniform",
                     help="uniform: the headline line (README scale); clustered: persistent schedule and captured "
                          "steps; learned: index forms on clustered data; serving: the request loop")
@@ -949,6 +955,8 @@ def main():
         w["nfiles"] = args.files
     if args.halos:
         w["nhalos"] = args.halos
+    if args.particles:
+        w["nparticles"] = args.particles
     if args.impl == "reference":
         # the reference is a CPU program: rank 0 alone runs it, other ranks exit
         if int(os.environ.get("RANK", "0")) != 0:
@@ -970,6 +978,8 @@ def main():
             w["nfiles"] = args.files
         if args.halos and "nhalos" in w:
             w["nhalos"] = args.halos
+        if args.particles:
+            w["nparticles"] = args.particles
         run = {"clustered": run_clustered, "learned": run_forms, "serving": run_serving}[args.workload]
         line = run(args, w, dist, rank, world, local)
         dist_close(dist)
