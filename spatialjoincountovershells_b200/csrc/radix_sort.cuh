@@ -31,8 +31,9 @@ constexpr int RS_WARPS = RS_THREADS / 32;
 constexpr int RS_BITS = 8;
 constexpr int RS_BINS = 1 << RS_BITS;
 constexpr int RS_SUBHIST = 4;  // upsweep: warps share RS_SUBHIST histograms
-// dynamic shared memory of the downsweep: exchanged keys + payloads
-constexpr size_t RS_DOWN_SMEM = (size_t)RS_TILE * (sizeof(uint32_t) + sizeof(uint4));
+// dynamic shared memory of the downsweep: exchanged keys + payloads, and for
+// array payloads the source slot of every ranked record
+constexpr size_t RS_DOWN_SMEM = (size_t)RS_TILE * (sizeof(uint32_t) + sizeof(uint4) + sizeof(uint16_t));
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -81,23 +82,57 @@ k_radix_upsweep(KeyOp kop, uint64_t n, int shift, uint32_t* __restrict__ hist, u
     }
 }
 
+// 16-byte asynchronous global -> shared copy (cp.async, L2 only); the copies
+// of a thread are awaited with cp_async_wait_all before a block barrier.
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gmem_src) {
+    const uint32_t d = (uint32_t)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(d), "l"(gmem_src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+template <class PayOp>
+struct PayIsArray {
+    static constexpr bool value = false;
+};
+template <>
+struct PayIsArray<PayFromArray> {
+    static constexpr bool value = true;
+};
+
 template <class KeyOp, class PayOp, class Sink>
 __global__ void __launch_bounds__(RS_THREADS)
 k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
                   const uint32_t* __restrict__ offs, uint32_t ntiles, Sink sink) {
+    // Array payloads are copied asynchronously into shared memory in load
+    // order as the tile starts, so their latency overlaps the ranking; the
+    // ranked records then carry their source slot.  Computed payloads are
+    // produced at the scatter, in rank order.
+    constexpr bool kAsync = PayIsArray<PayOp>::value;
     __shared__ uint32_t warp_cnt[RS_WARPS][RS_BINS];
     __shared__ uint32_t dstart[RS_BINS];
     __shared__ uint32_t gbase[RS_BINS];
     __shared__ uint32_t wsum[RS_BINS / 32];
     extern __shared__ uint4 xdyn[];
-    uint4* xpay = xdyn;                                            // [RS_TILE]
-    uint32_t* xkey = reinterpret_cast<uint32_t*>(xdyn + RS_TILE);  // [RS_TILE]
+    uint4* xpay = xdyn;                                            // [RS_TILE]: rank order, or load order (kAsync)
+    uint32_t* xkey = reinterpret_cast<uint32_t*>(xdyn + RS_TILE);  // [RS_TILE], rank order
+    uint16_t* xsrc = reinterpret_cast<uint16_t*>(xkey + RS_TILE);  // [RS_TILE], rank order (kAsync)
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
     const uint64_t tile_base = (uint64_t)tile * RS_TILE;
     const uint64_t rem = n - tile_base;
     const uint32_t tile_n = rem < (uint64_t)RS_TILE ? (uint32_t)rem : (uint32_t)RS_TILE;
+    const uint32_t wbase = (uint32_t)warp * 32u * RS_ITEMS;
+
+    if constexpr (kAsync) {
+#pragma unroll
+        for (int i = 0; i < RS_ITEMS; ++i) {
+            const uint32_t loc = wbase + (uint32_t)i * 32u + (uint32_t)lane;
+            if (loc < tile_n) cp_async16(&xpay[loc], pop.pay + tile_base + loc);
+        }
+    }
 
     for (int d = lane; d < RS_BINS; d += 32) warp_cnt[warp][d] = 0;
     __syncwarp();
@@ -106,7 +141,6 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
     // slot w*32*ITEMS + i*32 + l, so loads are coalesced and the stable order
     // inside the warp is item-major, lane-minor.
     uint32_t key[RS_ITEMS], pos[RS_ITEMS];
-    const uint32_t wbase = (uint32_t)warp * 32u * RS_ITEMS;
     const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int i = 0; i < RS_ITEMS; ++i) {
@@ -159,9 +193,11 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
             pos[i] += dstart[d] + warp_cnt[warp][d];
             const uint32_t loc = wbase + (uint32_t)i * 32u + (uint32_t)lane;
             xkey[pos[i]] = key[i];
-            xpay[pos[i]] = pop(tile_base + loc);
+            if constexpr (kAsync) xsrc[pos[i]] = (uint16_t)loc;
+            else xpay[pos[i]] = pop(tile_base + loc);
         }
     }
+    if constexpr (kAsync) cp_async_wait_all();
     __syncthreads();
 #pragma unroll
     for (int k = 0; k < RS_ITEMS; ++k) {
@@ -169,7 +205,7 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
         if (j < tile_n) {
             const uint32_t kk = xkey[j];
             const uint32_t d = (kk >> shift) & (RS_BINS - 1);
-            sink(gbase[d] + (j - dstart[d]), kk, xpay[j]);
+            sink(gbase[d] + (j - dstart[d]), kk, kAsync ? xpay[xsrc[j]] : xpay[j]);
         }
     }
 }
