@@ -177,17 +177,17 @@ __device__ __forceinline__ void count_shifted_images(const CountParams& p, const
 
 // Per-halo plan written by the planning phase (one lane per halo).
 struct HaloPlan {
-    float cx, cy, cz;
-    float lox, hix, loy, hiy, loz, hiz;
+    float cx, cy, cz;  // the box is c -+ half, recomputed (same fp32 ops) when the halo is counted
     uint32_t row;    // the halo's row in the count array
     uint32_t nrows;  // rows stored in the row list; kSlowPlan: count in place
     uint32_t flags;  // periodic axes whose box crosses a face (bit a = axis a)
 };
 constexpr uint32_t kSlowPlan = 0xffffffffu;
 constexpr int kBatch = 32;    // halos per warp batch (one per lane while planning)
-constexpr int kMaxRows = 28;  // rows kept per halo (a box spans <= 5x5 rows when cells are >= R/2)
+constexpr int kMaxRows = 25;  // rows kept per halo (a box spans <= 5x5 rows when cells are >= R/2)
 
-// Shared memory of one warp: plans and row lists of its current batch.
+// Shared memory of one warp: plans and row lists of its current batch (24 B
+// plans and 25-row lists keep a block at ~25 KB, so 8 blocks fit an SM).
 struct WarpPlans {
     HaloPlan plan[kBatch];
     uint32_t row_cell[kBatch][kMaxRows];  // cell-table index of the row's first cell
@@ -202,12 +202,6 @@ __device__ __forceinline__ void plan_halo(const CountParams& p, float4 c, bool v
     pl->cx = im.cx;
     pl->cy = im.cy;
     pl->cz = im.cz;
-    pl->lox = im.lox;
-    pl->hix = im.hix;
-    pl->loy = im.loy;
-    pl->hiy = im.hiy;
-    pl->loz = im.loz;
-    pl->hiz = im.hiz;
     pl->row = __float_as_uint(c.w);
     uint32_t F = 0;
     if (p.periodic)
@@ -310,12 +304,12 @@ __device__ __forceinline__ void count_batch(const CountParams& p, WarpPlans* wp,
         im.cx = pl.cx;
         im.cy = pl.cy;
         im.cz = pl.cz;
-        im.lox = pl.lox;
-        im.hix = pl.hix;
-        im.loy = pl.loy;
-        im.hiy = pl.hiy;
-        im.loz = pl.loz;
-        im.hiz = pl.hiz;
+        im.lox = __fsub_rn(pl.cx, p.half);
+        im.hix = __fadd_rn(pl.cx, p.half);
+        im.loy = __fsub_rn(pl.cy, p.half);
+        im.hiy = __fadd_rn(pl.cy, p.half);
+        im.loz = __fsub_rn(pl.cz, p.half);
+        im.hiz = __fadd_rn(pl.cz, p.half);
         if (pl.nrows == kSlowPlan) {
             count_image<BIN, BIG>(p, make_image(p, pl.cx, pl.cy, pl.cz), 0, sink, tab, lut, lane);
         } else {
