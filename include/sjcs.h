@@ -193,6 +193,19 @@ int sjcs_index_build(sjcs_ctx *ctx, const float *xyz, uint64_t n,
 /* Same, with the particles already in device memory (d_xyz, n*3 floats). */
 int sjcs_index_build_device(sjcs_ctx *ctx, const float *d_xyz, uint64_t n,
                             const sjcs_index_opts *opts, sjcs_index **out);
+/* Same, from compressed (Gadget-encoded) particles: n uint16 triplets in HOST
+ * memory (the displacement record of a compressed file) and the file's
+ * 256-byte header (the layout of GadgetHeader, include/Gadget/GadgetHeader.h:4-27;
+ * sjcs_gadget_header in sjcs_host.h).  The triplets are copied to the device
+ * and decoded there.  Replaces the decode loop of
+ * constructIndexWithSameThreadPool (src/astr_rcount/main.c:739-763:
+ * decodeCompressedParticle per particle, src/Gadget/BufVector3D.c:169-201)
+ * and the build. */
+int sjcs_index_build_compressed(sjcs_ctx *ctx, const uint16_t *uv, uint64_t n, const void *gadget_header,
+                                const sjcs_index_opts *opts, sjcs_index **out);
+/* Decode only, on the device: n triplets (host) into n x,y,z floats (host),
+ * exactly as decodeCompressedParticle computes them.  Blocks. */
+int sjcs_decode_compressed(sjcs_ctx *ctx, const uint16_t *uv, uint64_t n, const void *gadget_header, float *xyz);
 /* Block until the index is built. */
 int sjcs_index_wait(sjcs_index *idx);
 /* Number of particles in the index (getNumberOfDataArraySTR, ArraySTR.h:58). */

@@ -113,6 +113,48 @@ int sjcs_write_halo_file(const char *path, const sjcs_halo *h, uint64_t n);
 /* Write particles as a decoded particle file. */
 int sjcs_write_particle_file(const char *path, const float *xyz, uint64_t n);
 
+/* ---- compressed (Gadget-encoded) particle files --------------------------
+ * File: a Fortran record with the 256-byte header, then a record of
+ * npart[1] x 3 uint16 displacements (readCompressedParticles,
+ * src/Gadget/BufVector3D.c:110-135).  The header mirrors GadgetHeader
+ * (include/Gadget/GadgetHeader.h:4-27) field for field. */
+typedef struct sjcs_gadget_header {
+    int       npart[6];
+    double    mass[6];
+    double    time;
+    double    redshift;
+    int       flag_sfr;
+    int       flag_feedback;
+    int       npartTotal[6];
+    int       flag_cooling;
+    int       num_files;
+    double    BoxSize;
+    double    Omega0;
+    double    OmegaLambda;
+    double    HubbleParam;
+    int       flag_stellarage;
+    int       flag_metals;
+    int       hashsize;
+    float     disp_min;
+    float     disp_max;
+    int       pos_bits;
+    long long id_start;
+    long long id_end;
+    char      fill[56];
+} sjcs_gadget_header;
+/* Header only (readCompressedParticlesHeader, BufVector3D.c:90-108). */
+int sjcs_read_compressed_header(const char *path, sjcs_gadget_header *hdr);
+/* Header and the npart[1] uint16 triplets into uv (room for cap triplets). */
+int sjcs_read_compressed_particles(const char *path, sjcs_gadget_header *hdr, uint16_t *uv, uint64_t cap,
+                                   uint64_t *n);
+int sjcs_write_compressed_file(const char *path, const sjcs_gadget_header *hdr, const uint16_t *uv, uint64_t n);
+/* Synthetic compressed data (no real Gadget files are available): a lattice
+ * of n1d^3 particles (ids id_start ..), box `box`, displacements uniform in
+ * [0, 2^pos_bits) between disp_min and disp_max (MT19937 `seed`).  Fills hdr
+ * and the first n triplets (n <= n1d^3). */
+int sjcs_gen_compressed(uint32_t seed, int n1d, double box, float disp_min, float disp_max, int pos_bits,
+                        long long id_start, uint64_t n, sjcs_gadget_header *hdr, uint16_t *uv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -45,6 +45,7 @@ def lib():
         L.oracle_radius_table.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_int, vp]
         L.oracle_count.argtypes = [vp, u64, vp, ctypes.c_size_t, u64, vp, ctypes.c_int, ctypes.c_int, vp, ctypes.c_int]
         L.oracle_count_brute.argtypes = [vp, u64, vp, ctypes.c_size_t, u64, vp, ctypes.c_int, ctypes.c_int, vp]
+        L.oracle_decode_compressed.argtypes = [vp, vp, u64, vp]
         _lib = L
     return _lib
 
@@ -117,3 +118,25 @@ def ref_phase_times(stdout: str) -> dict:
     for m in re.finditer(r">>>> (.+?) time: (\d+) milli seconds", stdout):
         out[m.group(1)] = out.get(m.group(1), 0) + int(m.group(2))
     return out
+
+
+def decode_compressed(header_bytes: bytes, uv) -> np.ndarray:
+    """(n, 3) float32 positions of compressed particles (oracle restatement)."""
+    uv = np.ascontiguousarray(uv, dtype=np.uint16).reshape(-1, 3)
+    hdr = ctypes.create_string_buffer(bytes(header_bytes), 256)
+    out = np.empty((len(uv), 3), np.float32)
+    rc = lib().oracle_decode_compressed(hdr, uv.ctypes.data if len(uv) else None, len(uv),
+                                        out.ctypes.data if len(uv) else None)
+    if rc != 0:
+        raise ValueError("oracle_decode_compressed rejected the header")
+    return out
+
+
+REF_DECODE = REF_DIR / "ref_decode.exe"
+
+
+def ref_decode(path: str) -> np.ndarray:
+    """Positions of a compressed file decoded by the reference's own decoder
+    (oracle/ref_decode.c linked with its sources; test-fixture generation only)."""
+    r = subprocess.run([str(REF_DECODE), str(path)], capture_output=True, check=True)
+    return np.frombuffer(r.stdout, dtype=np.float32).reshape(-1, 3).copy()

@@ -345,3 +345,64 @@ int oracle_count_brute(const float *particles, uint64_t np, const float *halo_xy
         return -1;
     return run_all(img_brute, &b, halo_xyz, stride, nhalos, r2, nrads, periodic, counts, 1);
 }
+
+
+/* ---- compressed particles ----------------------------------------------- */
+
+typedef struct {
+    int npart[6];
+    double mass[6];
+    double time, redshift;
+    int flag_sfr, flag_feedback;
+    int npartTotal[6];
+    int flag_cooling, num_files;
+    double BoxSize, Omega0, OmegaLambda, HubbleParam;
+    int flag_stellarage, flag_metals, hashsize;
+    float disp_min, disp_max;
+    int pos_bits;
+    long long id_start, id_end;
+    char fill[56];
+} oracle_gadget_header;
+
+int oracle_decode_compressed(const void *header, const uint16_t *uv, uint64_t n, float *xyz)
+{
+    oracle_gadget_header h;
+    long long total, ng1d, ng2d, ng3d;
+    int n1d, nt1d = 1, nt2d = 1;
+    float cell_interval, span;
+    double unitsep;
+    uint64_t i;
+    if (!header || (n && (!uv || !xyz)))
+        return -1;
+    memcpy(&h, header, sizeof(h));
+    /* GadgetHeader.c:12-23, one tile */
+    total = (long long)h.npartTotal[1] + ((long long)h.npartTotal[2] << 32);
+    n1d = (int)pow((double)total + 0.5, 1 / 3.);
+    if (n1d <= 0)
+        return -1;
+    cell_interval = (float)(h.BoxSize / (double)n1d);
+    span = h.disp_max - h.disp_min;
+    unitsep = (double)span / pow(2.0, (double)h.pos_bits);
+    /* GadId.c:28-35: Ng2D is computed as an int product */
+    ng1d = n1d;
+    ng2d = (long long)(int)((unsigned)n1d * (unsigned)n1d);
+    ng3d = (long long)n1d * (long long)n1d * (long long)n1d;
+    for (i = 0; i < n; ++i) {
+        const long long ID = (long long)((unsigned long long)i + (unsigned long long)h.id_start);
+        const long long IDt = (ID - 1) / ng3d;                 /* IDall2IDpartGadId */
+        const long long IDg = ID - 1 - IDt * ng3d;
+        const int ig = (int)(IDg / ng2d);                      /* IDg2IndexGadId */
+        const int jg = (int)((IDg - ig * ng2d) / ng1d);
+        const int kg = (int)(IDg - ig * ng2d - jg * ng1d);
+        const int it = (int)(IDt / nt2d);                      /* IDt2IndexGadId */
+        const int jt = (int)((IDt - it * nt2d) / nt1d);
+        const int kt = (int)(IDt - it * nt2d - jt * nt1d);
+        const int ip[3] = {(int)(it * ng1d + ig), (int)(jt * ng1d + jg), (int)(kt * ng1d + kg)};
+        int a;
+        for (a = 0; a < 3; ++a) {
+            const float f = fmaf(cell_interval, (float)ip[a], h.disp_min);
+            xyz[3 * i + a] = (float)fma(unitsep, (double)uv[3 * i + a], (double)f);
+        }
+    }
+    return 0;
+}

@@ -37,6 +37,13 @@ int oracle_count(const float *particles, uint64_t np, const float *halo_xyz, siz
                  int nthreads);
 
 /* Same result, every particle tested against every image (tiny inputs only). */
+/* Decode n compressed particles (uint16 triplets, ids id_start + i) with the
+ * 256-byte Gadget header, restating decodeCompressedParticle
+ * (src/Gadget/BufVector3D.c:169-201), id2posGadId (src/Gadget/GadId.c:38-54,
+ * 80-146) and initGadgetDecodeParams (src/Gadget/GadgetHeader.c:9-24), in the
+ * contracted form the reference's -march build computes.  Returns 0 or -1. */
+int oracle_decode_compressed(const void *header, const uint16_t *uv, uint64_t n, float *xyz);
+
 int oracle_count_brute(const float *particles, uint64_t np, const float *halo_xyz, size_t stride,
                        uint64_t nhalos, const float *r2, int nrads, int periodic, uint64_t *counts);
 

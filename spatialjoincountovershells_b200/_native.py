@@ -103,6 +103,8 @@ _SIGS = {
     "sjcs_index_size": (_c.c_int, [_vp, _c.POINTER(_u64)]),
     "sjcs_index_grid": (_c.c_int, [_vp, _c.POINTER(_c.c_uint32)]),
     "sjcs_index_learned_info": (_c.c_int, [_vp, _c.POINTER(sjcs_learned_info)]),
+    "sjcs_index_build_compressed": (_c.c_int, [_vp, _vp, _u64, _vp, _c.POINTER(sjcs_index_opts), _pp]),
+    "sjcs_decode_compressed": (_c.c_int, [_vp, _vp, _u64, _vp, _vp]),
     "sjcs_step_create": (_c.c_int, [_vp, _vp, _vp, _u64, _c.POINTER(sjcs_index_opts), _pp]),
     "sjcs_step_launch": (_c.c_int, [_vp, _vp]),
     "sjcs_step_wait": (_c.c_int, [_vp]),
@@ -156,6 +158,11 @@ _HOST_SIGS = {
                                              _c.c_double, _c.c_double, _c.c_double, _c.c_uint32, _vp]),
     "sjcs_write_halo_file": (_c.c_int, [_c.c_char_p, _vp, _u64]),
     "sjcs_write_particle_file": (_c.c_int, [_c.c_char_p, _vp, _u64]),
+    "sjcs_read_compressed_header": (_c.c_int, [_c.c_char_p, _vp]),
+    "sjcs_read_compressed_particles": (_c.c_int, [_c.c_char_p, _vp, _vp, _u64, _c.POINTER(_u64)]),
+    "sjcs_write_compressed_file": (_c.c_int, [_c.c_char_p, _vp, _vp, _u64]),
+    "sjcs_gen_compressed": (_c.c_int, [_c.c_uint32, _c.c_int, _c.c_double, _c.c_float, _c.c_float, _c.c_int,
+                                       _c.c_longlong, _u64, _vp, _vp]),
 }
 
 
@@ -293,6 +300,27 @@ class Context:
                                           _c.byref(h)))
             keep = arr
         return Index(self, h, keep)
+
+    def build_index_compressed(self, uv, header: bytes, radius_hint: float = 0.0, kind: int = INDEX_GRID,
+                               level: int = 0) -> "Index":
+        """Index over compressed particles: (n, 3) uint16 displacements and the
+        file's 256-byte Gadget header; decoded on the device."""
+        uv = np.ascontiguousarray(uv, dtype=np.uint16).reshape(-1, 3)
+        hdr = _c.create_string_buffer(bytes(header), 256)
+        opts = _make_opts(radius_hint, None, kind, level, False)
+        h = _vp()
+        _check(lib().sjcs_index_build_compressed(self._h, _vp(uv.ctypes.data if len(uv) else 0), len(uv), hdr,
+                                                 _c.byref(opts), _c.byref(h)))
+        return Index(self, h, (uv, hdr))
+
+    def decode_compressed(self, uv, header: bytes) -> np.ndarray:
+        """(n, 3) float32 positions decoded on the device."""
+        uv = np.ascontiguousarray(uv, dtype=np.uint16).reshape(-1, 3)
+        out = np.empty((len(uv), 3), np.float32)
+        hdr = _c.create_string_buffer(bytes(header), 256)
+        _check(lib().sjcs_decode_compressed(self._h, _vp(uv.ctypes.data if len(uv) else 0), len(uv), hdr,
+                                            _vp(out.ctypes.data if len(uv) else 0)))
+        return out
 
     def step(self, query: "Query", n: int, radius_hint: float = 0.0, kind: int = INDEX_GRID, level: int = 0,
              verify: bool = False) -> "Step":
@@ -702,6 +730,36 @@ def gen_clustered_halos(seed: int, n: int, id0: int = 0, frac_at_clumps: float =
     _hcheck(host_lib().sjcs_gen_clustered_halos(seed, n, id0, p["nclumps"], p["sig_lo"], p["sig_hi"], p["wsig"],
                                                 frac_at_clumps, jitter, clump_seed, _vp(out.ctypes.data)))
     return out
+
+
+def gen_compressed(seed: int, n1d: int, box: float = 1000.0, disp_min: float = -4.0, disp_max: float = 4.0,
+                   pos_bits: int = 16, id_start: int = 1, n: int | None = None):
+    """Synthetic compressed particles: (256-byte header, (n, 3) uint16 displacements)."""
+    n = n1d ** 3 if n is None else n
+    hdr = _c.create_string_buffer(256)
+    uv = np.empty((n, 3), np.uint16)
+    _hcheck(host_lib().sjcs_gen_compressed(seed, n1d, box, disp_min, disp_max, pos_bits, id_start, n, hdr,
+                                           _vp(uv.ctypes.data if n else 0)))
+    return hdr.raw, uv
+
+
+def write_compressed_file(path, header: bytes, uv) -> None:
+    uv = np.ascontiguousarray(uv, dtype=np.uint16).reshape(-1, 3)
+    hdr = _c.create_string_buffer(bytes(header), 256)
+    _hcheck(host_lib().sjcs_write_compressed_file(os.fsencode(path), hdr, _vp(uv.ctypes.data if len(uv) else 0),
+                                                  len(uv)))
+
+
+def read_compressed(path):
+    """(256-byte header, (n, 3) uint16 displacements) of a compressed particle file."""
+    hdr = _c.create_string_buffer(256)
+    n = _u64()
+    _hcheck(host_lib().sjcs_read_compressed_particles(os.fsencode(path), hdr, None, 0, _c.byref(n)))
+    uv = np.empty((n.value, 3), np.uint16)
+    got = _u64()
+    _hcheck(host_lib().sjcs_read_compressed_particles(os.fsencode(path), hdr, _vp(uv.ctypes.data if n.value else 0),
+                                                      n.value, _c.byref(got)))
+    return hdr.raw, uv[: got.value]
 
 
 def write_halo_file(path, halos: np.ndarray) -> None:

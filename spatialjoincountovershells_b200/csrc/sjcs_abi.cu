@@ -568,6 +568,84 @@ int sjcs_index_build_device(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const
     return index_build_common(ctx, d_xyz, false, n, opts, out);
 }
 
+int sjcs_index_build_compressed(sjcs_ctx* ctx, const uint16_t* uv, uint64_t n, const void* gadget_header,
+                                const sjcs_index_opts* opts, sjcs_index** out) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!out) return fail(SJCS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (n && !uv) return fail(SJCS_ERR_INVALID, "uv is NULL");
+    if (n > 0xffffffffull) return fail(SJCS_ERR_INVALID, "too many particles for one index (%llu)", (unsigned long long)n);
+    GadgetDecode g{};
+    int rc = gadget_decode_params(gadget_header, &g);
+    if (rc) return rc;
+    sjcs_index_opts o{};
+    rc = check_opts(opts, &o);
+    if (rc) return rc;
+    rc = set_device(ctx);
+    if (rc) return rc;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    sjcs_index* idx = new_index(ctx);
+    if (!idx) return fail(SJCS_ERR_NOMEM, "out of host memory");
+    idx->kind = o.kind;
+    idx->n = n;
+    cudaStream_t s = ctx->s_build;
+    cudaEventRecord(idx->ev_start, s);
+    StreamScratch scr(s);
+    uint16_t* d_uv = nullptr;
+    float* d_xyz = nullptr;
+    cudaError_t e = scr.alloc(&d_uv, n * 3 * sizeof(uint16_t));
+    if (e == cudaSuccess) e = scr.alloc(&d_xyz, n * 3 * sizeof(float));
+    if (e != cudaSuccess) {
+        free_index(idx);
+        return fail(SJCS_ERR_NOMEM, "device allocation for %llu compressed particles failed: %s",
+                    (unsigned long long)n, cudaGetErrorString(e));
+    }
+    if (n) {
+        e = cudaMemcpyAsync(d_uv, uv, n * 3 * sizeof(uint16_t), cudaMemcpyHostToDevice, s);
+        if (e != cudaSuccess) {
+            free_index(idx);
+            return fail(SJCS_ERR_CUDA, "host-to-device copy failed: %s", cudaGetErrorString(e));
+        }
+        idx->had_h2d = true;
+    }
+    cudaEventRecord(idx->ev_h2d, s);
+    rc = launch_decode(d_uv, n, g, d_xyz, s);
+    if (!rc) rc = enqueue_build(ctx, idx, d_xyz, n, o, s);
+    if (rc) {
+        free_index(idx);
+        return rc;
+    }
+    cudaEventRecord(idx->ev_ready, s);
+    *out = idx;
+    return SJCS_OK;
+}
+
+int sjcs_decode_compressed(sjcs_ctx* ctx, const uint16_t* uv, uint64_t n, const void* gadget_header, float* xyz) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (n && (!uv || !xyz)) return fail(SJCS_ERR_INVALID, "uv or xyz is NULL");
+    GadgetDecode g{};
+    int rc = gadget_decode_params(gadget_header, &g);
+    if (rc) return rc;
+    rc = set_device(ctx);
+    if (rc) return rc;
+    if (n == 0) return SJCS_OK;
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t s = ctx->s_build;
+    {
+        StreamScratch scr(s);
+        uint16_t* d_uv = nullptr;
+        float* d_xyz = nullptr;
+        SJCS_CUDA_TRY(scr.alloc(&d_uv, n * 3 * sizeof(uint16_t)));
+        SJCS_CUDA_TRY(scr.alloc(&d_xyz, n * 3 * sizeof(float)));
+        SJCS_CUDA_TRY(cudaMemcpyAsync(d_uv, uv, n * 3 * sizeof(uint16_t), cudaMemcpyHostToDevice, s));
+        rc = launch_decode(d_uv, n, g, d_xyz, s);
+        if (rc) return rc;
+        SJCS_CUDA_TRY(cudaMemcpyAsync(xyz, d_xyz, n * 3 * sizeof(float), cudaMemcpyDeviceToHost, s));
+    }
+    SJCS_CUDA_TRY(cudaStreamSynchronize(s));
+    return SJCS_OK;
+}
+
 int sjcs_index_wait(sjcs_index* idx) {
     if (!valid_index(idx)) return fail(SJCS_ERR_STATE, "invalid index");
     SJCS_CUDA_TRY(cudaEventSynchronize(idx->ev_ready));

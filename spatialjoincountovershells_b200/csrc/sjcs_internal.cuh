@@ -201,6 +201,18 @@ struct Schedule;
 Schedule schedule_for(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx);
 Schedule resolve(const sjcs_schedule& in);
 
+// decode.cu: compressed (Gadget-encoded) particles
+struct GadgetDecode {
+    float cell_interval;  // BoxSize / n1d (fp32, as the reference stores it)
+    float disp_min;
+    double unitsep;       // (disp_max - disp_min) / 2^pos_bits
+    long long id_start;
+    long long ng1d, ng2d, ng3d;  // lattice per axis, per plane, total
+    int nt1d, nt2d;              // tiles (one)
+};
+int gadget_decode_params(const void* header, GadgetDecode* out);
+int launch_decode(const uint16_t* d_uv, uint64_t n, const GadgetDecode& g, float* d_xyz, cudaStream_t s);
+
 // query_prep.cu
 int sort_halos(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride_bytes, uint64_t nhalos,
                float4* out, cudaStream_t s);

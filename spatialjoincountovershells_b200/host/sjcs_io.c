@@ -645,3 +645,110 @@ out:
     free(total);
     return rc;
 }
+
+
+/* ---- compressed (Gadget-encoded) particle files --------------------------- */
+
+_Static_assert(sizeof(sjcs_gadget_header) == 256, "the Gadget header is 256 bytes");
+
+int sjcs_read_compressed_header(const char *path, sjcs_gadget_header *hdr)
+{
+    FILE *fp;
+    if (!path || !hdr)
+        return host_fail("invalid argument");
+    fp = fopen(path, "rb");
+    if (!fp)
+        return host_fail("ERROR: file %s not found in readCompressedParticlesHeader()", path);
+    if (fseek(fp, (long)sizeof(int), SEEK_SET) != 0 || fread(hdr, sizeof(*hdr), 1, fp) != 1) {
+        fclose(fp);
+        return host_fail("short read on %s (Gadget header)", path);
+    }
+    fclose(fp);
+    if (hdr->npart[1] < 0)
+        return host_fail("%s: negative particle count in the header", path);
+    return 0;
+}
+
+int sjcs_read_compressed_particles(const char *path, sjcs_gadget_header *hdr, uint16_t *uv, uint64_t cap,
+                                   uint64_t *n)
+{
+    FILE *fp;
+    uint64_t num;
+    if (!path || !hdr || !n)
+        return host_fail("invalid argument");
+    if (sjcs_read_compressed_header(path, hdr) != 0)
+        return -1;
+    num = (uint64_t)hdr->npart[1];
+    if (!uv) { /* count only */
+        *n = num;
+        return 0;
+    }
+    if (num > cap)
+        return host_fail("buffer holds %llu particles, file %s has %llu", (unsigned long long)cap, path,
+                         (unsigned long long)num);
+    fp = fopen(path, "rb");
+    if (!fp)
+        return host_fail("ERROR: file %s not found in readCompressedParticles()", path);
+    /* record marker, header, end marker + next record's marker */
+    if (fseek(fp, (long)(sizeof(int) + sizeof(*hdr) + 2 * sizeof(int)), SEEK_SET) != 0 ||
+        fread(uv, 3 * sizeof(uint16_t), (size_t)num, fp) != (size_t)num) {
+        fclose(fp);
+        return host_fail("short read on %s (compressed particles)", path);
+    }
+    fclose(fp);
+    *n = num;
+    return 0;
+}
+
+int sjcs_write_compressed_file(const char *path, const sjcs_gadget_header *hdr, const uint16_t *uv, uint64_t n)
+{
+    FILE *fp;
+    int m;
+    if (!path || !hdr || (n && !uv))
+        return host_fail("invalid argument");
+    fp = fopen(path, "wb");
+    if (!fp)
+        return host_fail("cannot create %s", path);
+    m = (int)sizeof(*hdr);
+    fwrite(&m, sizeof(m), 1, fp);
+    fwrite(hdr, sizeof(*hdr), 1, fp);
+    fwrite(&m, sizeof(m), 1, fp);
+    m = (int)(n * 3 * sizeof(uint16_t));
+    fwrite(&m, sizeof(m), 1, fp);
+    if (n)
+        fwrite(uv, 3 * sizeof(uint16_t), (size_t)n, fp);
+    fwrite(&m, sizeof(m), 1, fp);
+    if (fclose(fp) != 0)
+        return host_fail("write failed on %s", path);
+    return 0;
+}
+
+int sjcs_gen_compressed(uint32_t seed, int n1d, double box, float disp_min, float disp_max, int pos_bits,
+                        long long id_start, uint64_t n, sjcs_gadget_header *hdr, uint16_t *uv)
+{
+    sjcs_mt mt;
+    uint64_t i, total;
+    uint32_t mask;
+    if (!hdr || n1d <= 0 || pos_bits <= 0 || pos_bits > 16 || (n && !uv))
+        return host_fail("invalid argument");
+    total = (uint64_t)n1d * (uint64_t)n1d * (uint64_t)n1d;
+    if (n > total || n > 0x7fffffffull)
+        return host_fail("n (%llu) exceeds the lattice (%llu) or 2^31-1", (unsigned long long)n,
+                         (unsigned long long)total);
+    memset(hdr, 0, sizeof(*hdr));
+    hdr->npart[1] = (int)n;
+    hdr->npartTotal[1] = (int)(total & 0xffffffffull);
+    hdr->npartTotal[2] = (int)(total >> 32);
+    hdr->num_files = 1;
+    hdr->BoxSize = box;
+    hdr->disp_min = disp_min;
+    hdr->disp_max = disp_max;
+    hdr->pos_bits = pos_bits;
+    hdr->id_start = id_start;
+    hdr->id_end = id_start + (long long)n - 1;
+    mask = (pos_bits >= 16) ? 0xffffu : ((1u << pos_bits) - 1u);
+    sjcs_mt_seed(&mt, seed);
+    for (i = 0; i < 3 * n; ++i)
+        uv[i] = (uint16_t)(sjcs_mt_u32(&mt) & mask);
+    return 0;
+}

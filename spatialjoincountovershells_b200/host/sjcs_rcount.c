@@ -17,7 +17,9 @@
  * the build stream while the count stream searches the current one (the
  * reference's backlog pipeline, main.c:266-350, on two CUDA streams); a
  * missing or unreadable input file is reported and the program exits with
- * status 1 where the reference dereferences a NULL buffer.
+ * status 1 where the reference dereferences a NULL buffer.  --compressed
+ * files are read as uint16 triplets (half the bytes of decoded floats) and
+ * decoded on the GPU, bit-identically to decodeCompressedParticle.
  *
  * Added (GPU options, all optional): --index grid|morton|learned picks the
  * index form; --schedule auto|static|queue the count schedule; --autotune
@@ -143,6 +145,7 @@ static void die_lib(const char *what)
 
 static int g_index_kind = SJCS_INDEX_GRID;
 static bool g_autotune = false;
+static bool g_compressed = false; /* --compressed: Gadget-encoded particle files, decoded on the GPU */
 
 static void autotune_once(sjcs_ctx *ctx, sjcs_query *q, sjcs_index *idx)
 {
@@ -168,10 +171,33 @@ static void autotune_once(sjcs_ctx *ctx, sjcs_query *q, sjcs_index *idx)
 
 typedef struct Pending {
     int file;
-    float *host;
+    float *host; /* pinned: x,y,z floats, or uint16 triplets of a compressed file */
     uint64_t n;
     sjcs_index *idx;
 } Pending;
+
+/* A compressed file: header and triplets into pinned memory, then the build
+ * that decodes on the device (constructIndexWithSameThreadPool's compressed
+ * branch, src/astr_rcount/main.c:739-763). */
+static void start_index_compressed(sjcs_ctx *ctx, const char *fname, const sjcs_index_opts *opts, Pending *p)
+{
+    sjcs_gadget_header hdr;
+    uint64_t n = 0;
+    double t0 = now_us();
+    if (sjcs_read_compressed_particles(fname, &hdr, NULL, 0, &n) != 0) {
+        fprintf(stderr, "%s\n", sjcs_host_last_error());
+        exit(EXIT_FAILURE);
+    }
+    if (sjcs_host_alloc((n ? n : 1) * 3 * sizeof(uint16_t), (void **)&p->host) != SJCS_OK)
+        die_lib("pinned buffer");
+    if (sjcs_read_compressed_particles(fname, &hdr, (uint16_t *)p->host, n, &p->n) != 0) {
+        fprintf(stderr, "%s\n", sjcs_host_last_error());
+        exit(EXIT_FAILURE);
+    }
+    print_ms(">>>> particles reading time", t0);
+    if (sjcs_index_build_compressed(ctx, (const uint16_t *)p->host, p->n, &hdr, opts, &p->idx) != SJCS_OK)
+        die_lib("index build");
+}
 
 /* Read a particle file into pinned memory and queue its index build.
  * Replaces constructIndexWithSameThreadPool (main.c:732-786). */
@@ -183,6 +209,10 @@ static void start_index(sjcs_ctx *ctx, const char *fname, float radius_hint, Pen
     memset(&opts, 0, sizeof(opts));
     opts.kind = g_index_kind;
     opts.radius_hint = radius_hint;
+    if (g_compressed) {
+        start_index_compressed(ctx, fname, &opts, p);
+        return;
+    }
     t0 = now_us();
     if (sjcs_particle_file_count(fname, &n) != 0) {
         fprintf(stderr, "%s\n", sjcs_host_last_error());
@@ -206,7 +236,8 @@ static void finish_index(Pending *p, double t0)
     sjcs_host_free(p->host);
     p->host = NULL;
     if (t0 >= 0)
-        print_ms(">>>> index construction time", t0);
+        print_ms(g_compressed ? ">>>> particles decoding + index construction time" : ">>>> index construction time",
+                 t0);
     printf("  # of particles = %llu\n", (unsigned long long)p->n);
 }
 
@@ -552,9 +583,10 @@ int main(int argc, char *argv[])
         fprintf(stderr, "\n => %s\n", errmsg);
         usage_exit(argv);
     }
-    if (particle_compressed) {
-        fprintf(stderr, "ERROR: --compressed (Gadget-encoded) particle files are not supported by this build.\n");
-        exit(EXIT_FAILURE);
+    g_compressed = particle_compressed;
+    if (particle_compressed && use_graph) {
+        puts("  (--graph captures steps over decoded particle files; compressed files run uncaptured)");
+        use_graph = false;
     }
 
     /*** initialize ***/

@@ -107,6 +107,25 @@ def _c1(d: pathlib.Path) -> dict:
     return dict(particle_files=["c1_p.dat"], halo_file="c1_h.list", radius="0.001:5:40", threads=4)
 
 
+def _compressed(d: pathlib.Path) -> dict:
+    # Two compressed (Gadget-encoded) files of one 100^3 lattice, ids 1.. and
+    # 500001.., displacements in [-4, 4) at 16 bits; --compressed.
+    for k, (seed, id0) in enumerate([(41, 1), (42, 500_001)]):
+        hdr, uv = nat.gen_compressed(seed, 100, 1000.0, -4.0, 4.0, 16, id0, 500_000)
+        nat.write_compressed_file(d / f"cp_{k}.dat", hdr, uv)
+    h = np.concatenate([nat.gen_uniform_halos(43, 3000, 0), nat.gen_face_halos(44, 200, 3000, margin=5.0)])
+    nat.write_halo_file(d / "cp_h.list", h)
+    return dict(particle_files=["cp_0.dat", "cp_1.dat"], halo_file="cp_h.list", radius="0.001:5:40",
+                extra=["--compressed"], compressed=True)
+
+
+# Compressed decode vectors: (seed, n1d, box, disp_min, disp_max, pos_bits, id_start, n)
+DECODE_SETS = [(1, 60, 1000.0, -3.1, 4.7, 16, 7, None), (2, 37, 1000.0, -11.3, 9.9, 12, 0, 40000),
+               (3, 100, 999.7, 0.0, 2.5, 9, 123456, 300000), (4, 128, 1000.0, -6.0, 6.0, 16, 1, 200000)]
+
+# Cases whose particle files are compressed (run with --compressed).
+COMPRESSED_CASES = {"compressed": _compressed}
+
 CASES = {
     "kat": _kat,
     "uniform_small": _uniform_small,
@@ -120,7 +139,7 @@ CASES = {
 def materialize(name: str, d: pathlib.Path) -> dict:
     d = pathlib.Path(d)
     d.mkdir(parents=True, exist_ok=True)
-    spec = CASES[name](d)
+    spec = {**CASES, **COMPRESSED_CASES}[name](d)
     spec["nrads"] = int(spec["radius"].split(":")[-1])
     return spec
 
@@ -141,7 +160,10 @@ def load_halos_and_particles(spec: dict, d: pathlib.Path):
     extra = spec.get("extra", [])
     filt = d / extra[1] if "--filter-file" in extra else None
     halos = nat.read_halos(d / spec["halo_file"], filter_path=filt)
-    parts = [nat.read_particles(d / f) for f in spec["particle_files"]]
+    if spec.get("compressed"):
+        parts = [nat.read_compressed(d / f) for f in spec["particle_files"]]  # (header, uv) per file
+    else:
+        parts = [nat.read_particles(d / f) for f in spec["particle_files"]]
     return halos, parts
 
 

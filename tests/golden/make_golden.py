@@ -10,7 +10,10 @@ agrees byte for byte), and stores:
   golden/manifest.json  per case: command line, sha256 and size of the result text
   golden/kat_result.txt the full result text of the periodic known-answer case
 
-Usage:  python tests/golden/make_golden.py [case ...]
+  golden/compressed_decode.npz  the reference decoder's output for compressed
+                        particles (oracle/_ref/ref_decode.exe, see decode_vectors)
+
+Usage:  python tests/golden/make_golden.py [case ... | decode]
 """
 from __future__ import annotations
 
@@ -69,5 +72,26 @@ def main(names):
     man_path.write_text(json.dumps(manifest, indent=1, sort_keys=True) + "\n")
 
 
+def decode_vectors():
+    """golden/compressed_decode.npz: per decode set of cases.DECODE_SETS, the
+    sha256 of the reference decoder's float32 output (oracle/_ref/ref_decode.exe)
+    and its first 512 positions."""
+    from spatialjoincountovershells_b200 import _native as nat
+    shas, heads = [], []
+    for (seed, n1d, box, dmin, dmax, bits, id0, n) in cases.DECODE_SETS:
+        hdr, uv = nat.gen_compressed(seed, n1d, box, dmin, dmax, bits, id0, n)
+        with tempfile.TemporaryDirectory() as td:
+            f = pathlib.Path(td) / "c.dat"
+            nat.write_compressed_file(f, hdr, uv)
+            pos = oracle.ref_decode(f)
+        shas.append(hashlib.sha256(pos.tobytes()).hexdigest())
+        heads.append(pos[:512])
+        print(f"decode set {seed}: {len(pos)} particles")
+    np.savez_compressed(HERE / "compressed_decode.npz", sha256=np.array(shas), heads=np.stack(heads))
+
+
 if __name__ == "__main__":
-    main(sys.argv[1:] or list(cases.CASES))
+    names = sys.argv[1:] or [*cases.CASES, *cases.COMPRESSED_CASES, "decode"]
+    if "decode" in names:
+        decode_vectors()
+    main([n for n in names if n != "decode"])

@@ -47,7 +47,10 @@ def test_validation_matches_reference(args, built):
         assert (code, out, err) == (rcode, rout, rerr.replace(str(oracle.REF_ASTR), "PROG"))
 
 
-def test_compressed_is_refused_after_validation(tmp_path, built):
+def test_compressed_option_is_accepted(tmp_path, built):
+    # --compressed passes validation and reaches the run (which, without a
+    # GPU, stops at the device; the decode itself is tested on the GPU)
     code, out, err = _run(DRIVER, ["--thread", "1", "--next-setup", "1", "--radius", "0.1:1:4",
                                    "--particle-files", "p", "--halo-file", "h", "--compressed"])
-    assert code == 1 and "compressed = true" in out and "--compressed" in err
+    assert "compressed = true" in out and "not supported" not in err
+    assert code == 0 or (code == 1 and "ERROR:" in err)

@@ -10,7 +10,7 @@ from __future__ import annotations
 import numpy as np
 import pytest
 
-from conftest import golden_counts
+from conftest import GOLDEN, golden_counts
 from golden import cases
 from oracle import oracle
 from spatialjoincountovershells_b200 import _native as nat
@@ -84,3 +84,29 @@ def test_radius_labels_match_reference_text(built):
     want = ["  [0.0 ~ %f]: " % rad[0]] + ["  [%f ~ %f]: " % (rad[i - 1], rad[i]) for i in range(1, 40)]
     got = [ln[: ln.rindex(":") + 2] for ln in text[1:41]]
     assert got == want
+
+
+def test_compressed_decode_matches_the_reference_decoder():
+    # golden/compressed_decode.npz holds the output of the reference's own
+    # decodeCompressedParticle (oracle/_ref/ref_decode.exe) per decode set
+    import hashlib
+
+    from golden import cases
+    from spatialjoincountovershells_b200 import _native as nat
+    z = np.load(GOLDEN / "compressed_decode.npz")
+    for k, (seed, n1d, box, dmin, dmax, bits, id0, n) in enumerate(cases.DECODE_SETS):
+        hdr, uv = nat.gen_compressed(seed, n1d, box, dmin, dmax, bits, id0, n)
+        pos = oracle.decode_compressed(hdr, uv)
+        assert hashlib.sha256(pos.tobytes()).hexdigest() == z["sha256"][k], k
+        assert np.array_equal(pos[:512].view(np.uint32), z["heads"][k].view(np.uint32)), k
+
+
+def test_compressed_file_round_trip(tmp_path):
+    from spatialjoincountovershells_b200 import _native as nat
+    hdr, uv = nat.gen_compressed(9, 20, 500.0, -1.5, 2.5, 10, 11, 5000)
+    nat.write_compressed_file(tmp_path / "c.dat", hdr, uv)
+    h2, uv2 = nat.read_compressed(tmp_path / "c.dat")
+    assert h2 == hdr and np.array_equal(uv, uv2)
+    assert int.from_bytes(hdr[4:8], "little") == 5000           # npart[1]
+    assert int.from_bytes(hdr[100:104], "little") == 20 ** 3    # npartTotal[1]
+    assert (tmp_path / "c.dat").stat().st_size == 4 + 256 + 4 + 4 + 6 * 5000 + 4
