@@ -107,3 +107,20 @@ def test_schedule_arguments_are_validated(ctx):
         with pytest.raises(nat.SjcsError):
             q.set_schedule(**kw)
     q.destroy()
+
+
+def test_autotune_on_morton_indexes_keeps_static(ctx):
+    rng = np.random.default_rng(34)
+    p = rng.uniform(0, 1000, size=(50000, 3)).astype(np.float32)
+    h = rng.uniform(0, 1000, size=(2000, 3)).astype(np.float32)
+    r2 = nat.radius_table(0.001, 5, 40)
+    for kind in (nat.INDEX_MORTON, nat.INDEX_LEARNED):
+        idx = ctx.build_index(p, radius_hint=5.0, kind=kind)
+        q = ctx.query(h, r2)
+        res = ctx.autotune(q, idx)
+        assert len(res["trial_ms"]) == 1 and res["chosen"]["mode"] == nat.SCHED_STATIC
+        q.set_schedule(nat.SCHED_QUEUE)  # Morton forms count with the static schedule
+        q.count(idx)
+        assert np.array_equal(q.read_counts(), oracle.count(p, h, r2))
+        idx.destroy()
+        q.destroy()

@@ -112,3 +112,37 @@ def test_request_too_big_for_the_budget_is_refused(ctx, resident):
         # empty requests are fine
         out, info = srv.wait(srv.submit(np.zeros((0, 3), np.float32), nat.radius_table(0.1, 2, 8)))
         assert out.shape == (0, 8) and info["status"] == 0
+
+
+def test_server_over_learned_indexes_and_odd_tables(ctx):
+    rng = np.random.default_rng(74)
+    files = [rng.uniform(-5, 1005, size=(30000, 3)).astype(np.float32) for _ in range(2)]
+    files[0][:3] = [[np.nan, 1, 1], [np.inf, 2, 2], [0, 0, 0]]
+    idx = [ctx.build_index(f, radius_hint=10.0, kind=nat.INDEX_LEARNED, verify=True) for f in files]
+    h = rng.uniform(0, 1000, size=(700, 3)).astype(np.float32)
+    h[:4] = [[0, 0, 0], [1000, 1000, 1000], [np.nan, 5, 5], [999.99994, 0, 500]]
+    tables = [np.array([400.0, 100.0, 2500.0], np.float32), np.linspace(1, 3000, 2000).astype(np.float32),
+              nat.radius_table(0.01, 8.0, 33)]
+    with nat.Server(ctx, idx, slots=3) as srv:
+        tickets = [(srv.submit(h, r2, periodic=per), r2, per) for r2 in tables for per in (True, False)]
+        for t, r2, per in tickets:
+            out, info = srv.wait(t)
+            want = np.zeros((len(h), len(r2)), np.uint64)
+            for f in files:
+                oracle.count(f, h, r2, periodic=per, counts=want, brute=len(r2) < 10)
+            assert np.array_equal(out.astype(np.uint64), want), (r2[:3], per)
+    for i in idx:
+        i.destroy()
+
+
+def test_destroy_finishes_pending_requests(ctx, resident):
+    _, idx = resident
+    reqs = make_requests(75, 12)
+    srv = nat.Server(ctx, idx, slots=2)
+    outs = [np.zeros((len(hh), len(r2)), np.uint32) for hh, r2, _ in reqs]
+    for (hh, r2, per), o in zip(reqs, outs):
+        srv.submit(hh, r2, periodic=per, out=o)
+    srv.close()  # drains every submitted request before returning
+    with nat.Server(ctx, idx, slots=2) as s2:
+        for (hh, r2, per), o in zip(reqs, outs):
+            assert np.array_equal(s2.wait(s2.submit(hh, r2, periodic=per))[0], o)

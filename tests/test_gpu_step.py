@@ -11,6 +11,7 @@ import ctypes
 import numpy as np
 import pytest
 
+from oracle import oracle
 from spatialjoincountovershells_b200 import _native as nat
 
 pytestmark = pytest.mark.gpu
@@ -93,3 +94,45 @@ def test_driver_gpu_options_keep_the_reference_text(name, extra, case_dirs, mani
         assert "step time" in r.stdout
     if "--autotune" in extra:
         assert "autotune: schedule" in r.stdout
+
+
+def test_step_with_odd_tables_and_non_periodic_queries(ctx):
+    rng = np.random.default_rng(45)
+    n = 40000
+    files = [rng.uniform(0, 1000, size=(n, 3)).astype(np.float32) for _ in range(2)]
+    h = rng.uniform(0, 1000, size=(500, 3)).astype(np.float32)
+    h[:3] = [[0, 0, 0], [1000, 1000, 1000], [2, 998, 500]]
+    for r2, per in [(np.array([400.0, 100.0, 2500.0], np.float32), True),
+                    (np.linspace(1, 3000, 2000).astype(np.float32), False), (nat.radius_table(0.5, 30, 17), False)]:
+        q = ctx.query(h, r2, periodic=per)
+        st = ctx.step(q, n, radius_hint=10.0)
+        for f in files:
+            st.buffer[:] = f
+            st.launch().wait()
+        want = np.zeros((len(h), len(r2)), np.uint64)
+        for f in files:
+            oracle.count(f, h, r2, periodic=per, counts=want, brute=len(r2) < 10)
+        assert np.array_equal(q.read_counts(), want), (r2[:3], per)
+        st.destroy()
+        q.destroy()
+
+
+def test_driver_graph_with_files_of_different_sizes(tmp_path):
+    import hashlib
+    import subprocess
+
+    from test_gpu_parity import DRIVER
+    rng = np.random.default_rng(46)
+    sizes = [20000, 35000, 20000, 5000]
+    for k, m in enumerate(sizes):
+        nat.write_particle_file(tmp_path / f"p{k}.dat", rng.uniform(0, 1000, size=(m, 3)).astype(np.float32))
+    nat.write_halo_file(tmp_path / "h.list", nat.gen_uniform_halos(47, 800, 0))
+    outs = []
+    for extra in ([], ["--graph"]):
+        out = tmp_path / f"r{len(extra)}.txt"
+        args = ["--thread", "2", "--next-setup", "2", "--particle-files", *[f"p{k}.dat" for k in range(len(sizes))],
+                "--halo-file", "h.list", "--radius", "0.01:25:20", "--output-file", str(out), *extra]
+        r = subprocess.run([str(DRIVER), *args], cwd=tmp_path, capture_output=True, text=True, timeout=300)
+        assert r.returncode == 0, r.stderr
+        outs.append(hashlib.sha256(out.read_bytes()).hexdigest())
+    assert outs[0] == outs[1]
