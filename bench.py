@@ -683,14 +683,19 @@ def run_forms(args, w, dist, rank, world, local):
     parts_d = [torch.from_numpy(pnp[f * n:(f + 1) * n]).cuda() for f in range(nf)]
     halos_d = torch.from_numpy(hpts).cuda()
     torch.cuda.synchronize()
-    idx0 = ctx.build_index(parts_d[0], radius_hint=R)
-    qt = ctx.query(halos_d, r2)
-    tune = ctx.autotune(qt, idx0)
-    qt.destroy()
-    idx0.destroy()
+    # every form gets its own autotuned schedule (cached in the context per index kind)
+    tunes = {}
+    for kind in (nat.INDEX_GRID, nat.INDEX_MORTON, nat.INDEX_LEARNED):
+        idx0 = ctx.build_index(parts_d[0], radius_hint=R, kind=kind)
+        qt = ctx.query(halos_d, r2)
+        tunes[kind] = ctx.autotune(qt, idx0)
+        qt.destroy()
+        idx0.destroy()
+    tune = tunes[nat.INDEX_GRID]
 
     forms = [("grid", nat.INDEX_GRID, nat.SCHED_AUTO), ("grid-static", nat.INDEX_GRID, nat.SCHED_STATIC),
-             ("morton", nat.INDEX_MORTON, nat.SCHED_AUTO), ("learned", nat.INDEX_LEARNED, nat.SCHED_AUTO)]
+             ("morton", nat.INDEX_MORTON, nat.SCHED_AUTO), ("morton-static", nat.INDEX_MORTON, nat.SCHED_STATIC),
+             ("learned", nat.INDEX_LEARNED, nat.SCHED_AUTO), ("learned-static", nat.INDEX_LEARNED, nat.SCHED_STATIC)]
     K, W = args.steps, args.warmup
     res, ref_counts, info = {}, None, None
     for name, kind, mode in forms:
@@ -726,7 +731,8 @@ def run_forms(args, w, dist, rank, world, local):
         res[name] = {"value": round(nh * nf * world / (ms / 1e3), 1), "ms_per_step": round(ms, 3),
                      "build_s_per_file": round(statistics.mean(bts) / 1e3, 5),
                      "count_ms_per_file": round(count_ms, 3) if count_ms else None,
-                     "counts_identical_to_grid": same, "gpu_launches": launches, "clocks": clocks}
+                     "counts_identical_to_grid": same, "gpu_launches": launches, "clocks": clocks,
+                     "schedule": tunes[kind]["chosen"] if mode == nat.SCHED_AUTO else "static"}
     del ref_counts
     line = {
         "metric": METRIC, "value": res["learned"]["value"], "unit": UNIT, "n_gpus": world, "steps": K,

@@ -69,7 +69,7 @@ extern "C" {
 #define SJCS_SCHED_STATIC  1 /* warps take halos strided over the Morton order, in batches of 32 */
 #define SJCS_SCHED_QUEUE   2 /* persistent warps pull work from a queue ordered by estimated candidate
                                 count (largest first); heavy halos are split into pieces that several
-                                warps count together (grid index only; other kinds count STATIC) */
+                                warps count together (every index kind) */
 
 /* query flags */
 #define SJCS_QUERY_PERIODIC     0x1 /* periodic images, as multiRangeCountWithPriodicBoundArraySTR */

@@ -19,6 +19,7 @@
 
 #include "count_common.cuh"
 #include "morton.cuh"
+#include "queue_common.cuh"
 #include "sjcs_internal.cuh"
 
 namespace sjcs {
@@ -57,11 +58,22 @@ __device__ __forceinline__ int mcell_hi(const MortonParams& m, float v) {
     return (v != v) ? m.G - 1 : (int)(morton_q(v) >> m.sh);
 }
 
+// The candidates of up to 32 slot ranges: all of them, or piece `part` of
+// `nparts` (heavy halos shared by several warps of the queue schedule).
+template <int BIN, bool BIG>
+__device__ __forceinline__ void run_ranges(const CountParams& p, const Image& im, uint32_t s0, uint32_t s1,
+                                           uint32_t* __restrict__ sink, const float* __restrict__ tab,
+                                           const uint32_t* __restrict__ lut, int lane, uint32_t part, uint32_t nparts) {
+    if (nparts > 1) run_rows_part<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane, part, nparts);
+    else run_rows<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane);
+}
+
 template <int LOOK, int BIN, bool BIG>
 __device__ __forceinline__ void count_image_m(const CountParams& p, const MortonParams& m, const RootRegs& rr,
                                               float cx, float cy, float cz, uint32_t* __restrict__ sink,
                                               const float* __restrict__ tab, const uint32_t* __restrict__ lut,
-                                              uint2* __restrict__ pend, int lane) {
+                                              uint2* __restrict__ pend, int lane, uint32_t part = 0,
+                                              uint32_t nparts = 1) {
     Image im;
     im.cx = cx;
     im.cy = cy;
@@ -129,7 +141,7 @@ __device__ __forceinline__ void count_image_m(const CountParams& p, const Morton
                 if ((uint32_t)lane < npend - 32u) pend[lane] = pend[32 + lane];
                 __syncwarp();
                 npend -= 32u;
-                run_rows<BIN, BIG>(p, im, r.x, r.y, sink, tab, lut, lane);
+                run_ranges<BIN, BIG>(p, im, r.x, r.y, sink, tab, lut, lane, part, nparts);
             }
         }
     }
@@ -137,23 +149,118 @@ __device__ __forceinline__ void count_image_m(const CountParams& p, const Morton
         __syncwarp();
         const uint2 r = (uint32_t)lane < npend ? pend[lane] : make_uint2(0u, 0u);
         __syncwarp();
-        run_rows<BIN, BIG>(p, im, r.x, r.y, sink, tab, lut, lane);
+        run_ranges<BIN, BIG>(p, im, r.x, r.y, sink, tab, lut, lane, part, nparts);
     }
 }
 
+// One halo: every periodic image (MultiRangeCount.c:31-71), then the warp's
+// counters flushed into the halo's row.
 template <int LOOK, int BIN, bool BIG>
-__global__ void __launch_bounds__(MC_THREADS, 8) k_morton_count(CountParams p, MortonParams m) {
-    extern __shared__ uint32_t smem[];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    uint2* pend = reinterpret_cast<uint2*>(smem) + warp * kPend;
+__device__ __forceinline__ void count_halo_m(const CountParams& p, const MortonParams& m, const RootRegs& rr,
+                                             const float4 c, uint32_t* __restrict__ wcnt,
+                                             const float* __restrict__ tab, const uint32_t* __restrict__ lut,
+                                             uint2* __restrict__ pend, int lane, uint32_t part, uint32_t nparts) {
+    uint32_t* row = p.counts + (uint64_t)__float_as_uint(c.w) * (uint64_t)p.nrads;
+    uint32_t* sink = BIG ? row : wcnt;
+    count_image_m<LOOK, BIN, BIG>(p, m, rr, c.x, c.y, c.z, sink, tab, lut, pend, lane, part, nparts);
+    if (p.periodic) {
+        const float lox = __fsub_rn(c.x, p.half), hix = __fadd_rn(c.x, p.half);
+        const float loy = __fsub_rn(c.y, p.half), hiy = __fadd_rn(c.y, p.half);
+        const float loz = __fsub_rn(c.z, p.half), hiz = __fadd_rn(c.z, p.half);
+        const unsigned F = ((lox < kBoxLow) | (hix > kBoxUpp) ? 1u : 0u) |
+                           ((loy < kBoxLow) | (hiy > kBoxUpp) ? 2u : 0u) |
+                           ((loz < kBoxLow) | (hiz > kBoxUpp) ? 4u : 0u);
+        if (F) {
+            // min_oob takes precedence over max_oob on an axis (MultiRangeCount.c:38-43)
+            const float sx = (lox < kBoxLow) ? __fadd_rn(c.x, kBoxUpp) : __fsub_rn(c.x, kBoxUpp);
+            const float sy = (loy < kBoxLow) ? __fadd_rn(c.y, kBoxUpp) : __fsub_rn(c.y, kBoxUpp);
+            const float sz = (loz < kBoxLow) ? __fadd_rn(c.z, kBoxUpp) : __fsub_rn(c.z, kBoxUpp);
+            for (unsigned S = F; S != 0; S = (S - 1u) & F)
+                count_image_m<LOOK, BIN, BIG>(p, m, rr, (S & 1u) ? sx : c.x, (S & 2u) ? sy : c.y,
+                                              (S & 4u) ? sz : c.z, sink, tab, lut, pend, lane, part, nparts);
+        }
+    }
+    if (!BIG) {
+        __syncwarp();
+        for (int sh = lane; sh < p.nrads; sh += 32) {
+            const uint32_t v = wcnt[sh];
+            if (v) {
+                wcnt[sh] = 0u;
+                atomicAdd(row + sh, v);  // result unused: compiles to a reduction
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Shared-memory set-up common to both schedules and the root model in registers.
+struct MView {
+    uint2* pend;
+    const float* tab;
+    const uint32_t* lut;
+    uint32_t* wcnt;
+    RootRegs rr;
+};
+
+template <int LOOK, bool BIG>
+__device__ __forceinline__ MView setup_m(const CountParams& p, const MortonParams& m, uint32_t* smem, int tid,
+                                         int warp) {
+    MView v;
+    v.pend = reinterpret_cast<uint2*>(smem) + warp * kPend;
     float* r2s = reinterpret_cast<float*>(reinterpret_cast<uint2*>(smem) + MC_WARPS * kPend);
     uint32_t* luts = reinterpret_cast<uint32_t*>(r2s + p.pad);
-    uint32_t* wcnt = luts + p.nlut + warp * p.nrads;
+    v.wcnt = luts + p.nlut + warp * p.nrads;
     if (!BIG) {
         for (int i = tid; i < p.pad; i += MC_THREADS) r2s[i] = p.r2[i];
         for (int i = tid; i < p.nlut; i += MC_THREADS) luts[i] = p.lut[i];
         for (int i = tid; i < MC_WARPS * p.nrads; i += MC_THREADS) luts[p.nlut + i] = 0u;
     }
+    v.rr = RootRegs{};
+    if (LOOK == LOOK_MODEL) {
+        v.rr.kmin = m.root->kmin;
+        v.rr.kmax = m.root->kmax;
+        v.rr.shift = m.root->shift;
+        v.rr.n = m.root->n;
+        v.rr.table_only = m.root->mismatches != 0ull;
+    }
+    v.tab = BIG ? p.r2 : r2s;
+    v.lut = BIG ? p.lut : luts;
+    return v;
+}
+
+// Static schedule: warp gw of W takes halos gw, gw + W, ... (the resident
+// warps work on one window of the Morton order and share particle lines).
+template <int LOOK, int BIN, bool BIG>
+__global__ void __launch_bounds__(MC_THREADS, 8) k_morton_count(CountParams p, MortonParams m) {
+    extern __shared__ uint32_t smem[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const MView v = setup_m<LOOK, BIG>(p, m, smem, tid, warp);
+    __syncthreads();
+    const uint64_t W = (uint64_t)gridDim.x * MC_WARPS;
+    for (uint64_t hk = (uint64_t)blockIdx.x * MC_WARPS + warp; hk < p.nhalos; hk += W)
+        count_halo_m<LOOK, BIN, BIG>(p, m, v.rr, p.halos[hk], v.wcnt, v.tab, v.lut, v.pend, lane, 0, 1);
+}
+
+// Rank of a cell boundary at any level <= 10 (queue estimates): the table
+// covers the index's level L, so a coarser cell c' starts at table[c' * 8^(L-l)].
+template <int LOOK>
+__device__ __forceinline__ uint32_t rank_at(const MortonParams& m, const RootRegs& rr, uint32_t code, int up) {
+    if (LOOK == LOOK_TABLE || rr.table_only) return __ldg(m.table + ((uint64_t)code << (3 * up)));
+    LearnedRoot rt;
+    rt.kmin = rr.kmin;
+    rt.kmax = rr.kmax;
+    rt.shift = rr.shift;
+    rt.n = rr.n;
+    return learned_rank(rt, m.leaves, m.wpref, (unsigned long long)code << (m.key_shift + 3 * up));
+}
+
+// Queue estimate (lane per halo): particles in the halo's box of cells one
+// level coarser than the index's (x 2^k for k periodic axes), from the same
+// ranks the count uses (offset table or learned model).
+template <int LOOK>
+__global__ void k_estimate_m(CountParams p, MortonParams m, uint32_t* __restrict__ key, uint32_t* __restrict__ hist) {
+    __shared__ uint32_t sh[kBuckets];
+    for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) sh[i] = 0;
     RootRegs rr{};
     if (LOOK == LOOK_MODEL) {
         rr.kmin = m.root->kmin;
@@ -163,41 +270,70 @@ __global__ void __launch_bounds__(MC_THREADS, 8) k_morton_count(CountParams p, M
         rr.table_only = m.root->mismatches != 0ull;
     }
     __syncthreads();
-    const float* tab = BIG ? p.r2 : r2s;
-    const uint32_t* lut = BIG ? p.lut : luts;
-    const uint64_t W = (uint64_t)gridDim.x * MC_WARPS;
-    for (uint64_t hk = (uint64_t)blockIdx.x * MC_WARPS + warp; hk < p.nhalos; hk += W) {
-        const float4 c = p.halos[hk];
-        uint32_t* row = p.counts + (uint64_t)__float_as_uint(c.w) * (uint64_t)p.nrads;
-        uint32_t* sink = BIG ? row : wcnt;
-        count_image_m<LOOK, BIN, BIG>(p, m, rr, c.x, c.y, c.z, sink, tab, lut, pend, lane);
-        if (p.periodic) {
-            const float lox = __fsub_rn(c.x, p.half), hix = __fadd_rn(c.x, p.half);
-            const float loy = __fsub_rn(c.y, p.half), hiy = __fadd_rn(c.y, p.half);
-            const float loz = __fsub_rn(c.z, p.half), hiz = __fadd_rn(c.z, p.half);
-            const unsigned F = ((lox < kBoxLow) | (hix > kBoxUpp) ? 1u : 0u) |
-                               ((loy < kBoxLow) | (hiy > kBoxUpp) ? 2u : 0u) |
-                               ((loz < kBoxLow) | (hiz > kBoxUpp) ? 4u : 0u);
-            if (F) {
-                // min_oob takes precedence over max_oob on an axis (MultiRangeCount.c:38-43)
-                const float sx = (lox < kBoxLow) ? __fadd_rn(c.x, kBoxUpp) : __fsub_rn(c.x, kBoxUpp);
-                const float sy = (loy < kBoxLow) ? __fadd_rn(c.y, kBoxUpp) : __fsub_rn(c.y, kBoxUpp);
-                const float sz = (loz < kBoxLow) ? __fadd_rn(c.z, kBoxUpp) : __fsub_rn(c.z, kBoxUpp);
-                for (unsigned S = F; S != 0; S = (S - 1u) & F)
-                    count_image_m<LOOK, BIN, BIG>(p, m, rr, (S & 1u) ? sx : c.x, (S & 2u) ? sy : c.y,
-                                                  (S & 4u) ? sz : c.z, sink, tab, lut, pend, lane);
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < p.nhalos) {
+        const float4 c = p.halos[i];
+        const int up = m.G > 1 ? 1 : 0;  // one level coarser
+        const int sh2 = m.sh + up, G2 = m.G >> up;
+        const float lo[3] = {__fsub_rn(c.x, p.half), __fsub_rn(c.y, p.half), __fsub_rn(c.z, p.half)};
+        const float hi[3] = {__fadd_rn(c.x, p.half), __fadd_rn(c.y, p.half), __fadd_rn(c.z, p.half)};
+        int a0[3], a1[3];
+        uint64_t ncell = 1;
+        for (int a = 0; a < 3; ++a) {
+            a0[a] = (int)(morton_q(lo[a]) >> sh2);
+            a1[a] = (hi[a] != hi[a]) ? G2 - 1 : (int)(morton_q(hi[a]) >> sh2);
+            ncell *= (uint64_t)(a1[a] - a0[a] + 1);
+        }
+        uint64_t e = 0;
+        if (ncell > 64) {
+            e = 0x40000000ull;  // huge box: certainly heavy
+        } else {
+            for (int z = a0[2]; z <= a1[2]; ++z)
+                for (int y = a0[1]; y <= a1[1]; ++y)
+                    for (int x = a0[0]; x <= a1[0]; ++x) {
+                        const uint32_t code = morton_cell((uint32_t)x, (uint32_t)y, (uint32_t)z);
+                        e += rank_at<LOOK>(m, rr, code + 1u, up) - rank_at<LOOK>(m, rr, code, up);
+                    }
+            if (p.periodic) {
+                const int k = ((lo[0] < kBoxLow) | (hi[0] > kBoxUpp)) + ((lo[1] < kBoxLow) | (hi[1] > kBoxUpp)) +
+                              ((lo[2] < kBoxLow) | (hi[2] > kBoxUpp));
+                e <<= k;
             }
         }
-        if (!BIG) {
-            __syncwarp();
-            for (int sh = lane; sh < p.nrads; sh += 32) {
-                const uint32_t v = wcnt[sh];
-                if (v) {
-                    wcnt[sh] = 0u;
-                    atomicAdd(row + sh, v);  // result unused: compiles to a reduction
-                }
-            }
-            __syncwarp();
+        const uint32_t ev = e < 0x40000000ull ? (uint32_t)e : 0x40000000u;
+        const uint32_t k = 255u - est_bucket(ev);
+        key[i] = k;
+        atomicAdd(&sh[k], 1u);
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < kBuckets; k += blockDim.x)
+        if (sh[k]) atomicAdd(hist + k, sh[k]);
+}
+
+// Queue schedule: persistent warps claim items (batches of light halos, or
+// pieces of heavy ones) largest first.
+template <int LOOK, int BIN, bool BIG>
+__global__ void __launch_bounds__(MC_THREADS, 8) k_morton_count_queue(CountParams p, MortonParams m, QueueParams q) {
+    extern __shared__ uint32_t smem[];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const MView v = setup_m<LOOK, BIG>(p, m, smem, tid, warp);
+    __syncthreads();
+    const uint32_t nitems = q.ctl[1];
+    int bk = 0;
+    for (;;) {
+        BucketPlan bp;
+        uint32_t r;
+        if (!claim_item(q, nitems, lane, &bk, &bp, &r)) break;
+        if (bp.per == 0) {
+            const uint32_t pos = bp.start + r / bp.pieces, part = r % bp.pieces;
+            count_halo_m<LOOK, BIN, BIG>(p, m, v.rr, p.halos[q.ord[pos]], v.wcnt, v.tab, v.lut, v.pend, lane, part,
+                                         bp.pieces);
+        } else {
+            const uint32_t first = r * bp.per;
+            const uint32_t nb = min(bp.per, bp.count - first);
+            for (uint32_t k = 0; k < nb; ++k)
+                count_halo_m<LOOK, BIN, BIG>(p, m, v.rr, p.halos[q.ord[bp.start + first + k]], v.wcnt, v.tab, v.lut,
+                                             v.pend, lane, 0, 1);
         }
     }
 }
@@ -217,25 +353,65 @@ int launch_m(sjcs_ctx* ctx, const CountParams& p, const MortonParams& m, size_t 
     return SJCS_OK;
 }
 
+template <int LOOK, int BIN, bool BIG>
+int launch_mq(sjcs_ctx* ctx, const CountParams& p, const MortonParams& m, const Schedule& sc, size_t smem,
+              cudaStream_t s) {
+    const uint64_t n = p.nhalos;
+    if (n * (uint64_t)sc.max_pieces >= (1ull << 32))
+        return fail(SJCS_ERR_INVALID, "queue schedule: nhalos * max_pieces must stay below 2^32");
+    const uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
+    StreamScratch scr(s);  // freed (stream-ordered) after the kernels below
+    uint32_t *key, *ord, *ctl, *hist, *rhist;
+    BucketPlan* plan;
+    SJCS_CUDA_TRY(scr.alloc(&key, n * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&ord, n * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&ctl, 4 * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&hist, kBuckets * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&plan, kBuckets * sizeof(BucketPlan)));
+    SJCS_CUDA_TRY(scr.alloc(&rhist, (uint64_t)RS_BINS * ntiles * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(cudaMemsetAsync(hist, 0, kBuckets * sizeof(uint32_t), s));
+    k_estimate_m<LOOK><<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, m, key, hist);
+    SJCS_LAUNCH_CHECK();
+    int rc = order_and_plan(n, key, hist, sc, ord, plan, ctl, rhist, s);
+    if (rc) return rc;
+    auto kern = k_morton_count_queue<LOOK, BIN, BIG>;
+    if (smem > 48 * 1024)
+        SJCS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    SJCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, MC_THREADS, smem));
+    if (per_sm < 1) per_sm = 1;
+    kern<<<(unsigned)(ctx->num_sms * per_sm), MC_THREADS, smem, s>>>(p, m, QueueParams{ord, plan, ctl});
+    SJCS_LAUNCH_CHECK();
+    return SJCS_OK;
+}
+
+template <int LOOK, int BIN, bool BIG>
+int launch_sched(sjcs_ctx* ctx, const CountParams& p, const MortonParams& m, const Schedule* sc, size_t smem,
+                 cudaStream_t s) {
+    if (sc && sc->mode == SJCS_SCHED_QUEUE) return launch_mq<LOOK, BIN, BIG>(ctx, p, m, *sc, smem, s);
+    return launch_m<LOOK, BIN, BIG>(ctx, p, m, smem, s);
+}
+
 template <int LOOK>
 int dispatch_bin(sjcs_ctx* ctx, int bin, bool big, const CountParams& p, const MortonParams& m, size_t smem,
-                 cudaStream_t s) {
+                 cudaStream_t s, const Schedule* sc) {
     switch (bin) {
         case BIN_LUT:
-            return big ? launch_m<LOOK, BIN_LUT, true>(ctx, p, m, smem, s)
-                       : launch_m<LOOK, BIN_LUT, false>(ctx, p, m, smem, s);
+            return big ? launch_sched<LOOK, BIN_LUT, true>(ctx, p, m, sc, smem, s)
+                       : launch_sched<LOOK, BIN_LUT, false>(ctx, p, m, sc, smem, s);
         case BIN_BSEARCH:
-            return big ? launch_m<LOOK, BIN_BSEARCH, true>(ctx, p, m, smem, s)
-                       : launch_m<LOOK, BIN_BSEARCH, false>(ctx, p, m, smem, s);
+            return big ? launch_sched<LOOK, BIN_BSEARCH, true>(ctx, p, m, sc, smem, s)
+                       : launch_sched<LOOK, BIN_BSEARCH, false>(ctx, p, m, sc, smem, s);
         default:
-            return big ? launch_m<LOOK, BIN_FIRST_MATCH, true>(ctx, p, m, smem, s)
-                       : launch_m<LOOK, BIN_FIRST_MATCH, false>(ctx, p, m, smem, s);
+            return big ? launch_sched<LOOK, BIN_FIRST_MATCH, true>(ctx, p, m, sc, smem, s)
+                       : launch_sched<LOOK, BIN_FIRST_MATCH, false>(ctx, p, m, sc, smem, s);
     }
 }
 
 }  // namespace
 
-int launch_morton_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s) {
+int launch_morton_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s,
+                        const Schedule* sc) {
     if (q->nhalos == 0 || idx->n == 0) return SJCS_OK;
     CountParams p{};
     p.pts = idx->pts;
@@ -270,8 +446,8 @@ int launch_morton_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* id
                         (big ? 0 : (size_t)(q->pad + q->nlut + MC_WARPS * q->nrads) * sizeof(uint32_t));
     // Learned kind: model lookups, unless the judge recorded a mismatch (the
     // kernel reads the record and then answers from the table).
-    return idx->kind == SJCS_INDEX_LEARNED ? dispatch_bin<LOOK_MODEL>(ctx, bin, big, p, m, smem, s)
-                 : dispatch_bin<LOOK_TABLE>(ctx, bin, big, p, m, smem, s);
+    return idx->kind == SJCS_INDEX_LEARNED ? dispatch_bin<LOOK_MODEL>(ctx, bin, big, p, m, smem, s, sc)
+                                           : dispatch_bin<LOOK_TABLE>(ctx, bin, big, p, m, smem, s, sc);
 }
 
 }  // namespace sjcs

@@ -128,7 +128,7 @@ int enqueue(sjcs_server* srv, Slot& sl) {
         for (const sjcs_index* ix : srv->idx) {
             const Schedule sc = schedule_for(srv->ctx, &sl.q, ix);
             rc = ix->kind == SJCS_INDEX_GRID ? launch_shell_count(srv->ctx, &sl.q, ix, s, &sc)
-                                             : launch_morton_count(srv->ctx, &sl.q, ix, s);
+                                             : launch_morton_count(srv->ctx, &sl.q, ix, s, &sc);
             if (rc) return rc;
         }
     }

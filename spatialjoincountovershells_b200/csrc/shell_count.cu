@@ -38,6 +38,7 @@
 // back before the square root; the x cell range then uses cx -+ (xr + 1e-3 +
 // 1e-6*(|cx| + xr)).
 #include "count_common.cuh"
+#include "queue_common.cuh"
 #include "radix_sort.cuh"
 #include "sjcs_internal.cuh"
 
@@ -385,27 +386,6 @@ __global__ void __launch_bounds__(CT_THREADS, 8) k_shell_count(CountParams p) {
 //               claim ever fails or retries), largest buckets first, so the
 //               longest items start early and the light ones fill the tail.
 
-struct BucketPlan {
-    uint32_t start;   // first position of the bucket in ord
-    uint32_t count;   // halos in the bucket
-    uint32_t per;     // halos per item (batch) or 0 when halos are split
-    uint32_t pieces;  // pieces per halo when split
-    uint32_t item0;   // first item of the bucket
-};
-constexpr int kBuckets = 256;
-
-struct QueueParams {
-    const uint32_t* __restrict__ ord;     // Morton index, descending size buckets
-    const BucketPlan* __restrict__ plan;  // [kBuckets] in position order (key 0 = largest)
-    uint32_t* __restrict__ ctl;           // [0] item counter, [1] total items
-};
-
-__device__ __forceinline__ uint32_t bucket_low(uint32_t b) {
-    if (b == 0) return 0u;
-    const uint32_t lg = (b - 1u) >> 3, mant = (b - 1u) & 7u;
-    return lg >= 3 ? (8u + mant) << (lg - 3) : (8u + mant) >> (3 - lg);
-}
-
 __global__ void k_estimate(CountParams p, uint32_t* __restrict__ key, uint32_t* __restrict__ hist) {
     __shared__ uint32_t sh[kBuckets];
     for (int i = threadIdx.x; i < kBuckets; i += blockDim.x) sh[i] = 0;
@@ -455,40 +435,6 @@ __global__ void k_estimate(CountParams p, uint32_t* __restrict__ key, uint32_t* 
         if (sh[k]) atomicAdd(hist + k, sh[k]);
 }
 
-// One block of kBuckets threads: bucket starts, item sizes and item prefix.
-__global__ void k_plan_items(const uint32_t* __restrict__ hist, uint32_t piece, uint32_t max_pieces,
-                             uint32_t single, BucketPlan* __restrict__ plan, uint32_t* __restrict__ ctl) {
-    __shared__ uint32_t s_cnt[kBuckets], s_items[kBuckets];
-    const int k = threadIdx.x;  // position order: key k holds bucket 255 - k
-    const uint32_t cnt = hist[k];
-    const uint32_t lo = bucket_low(255u - (uint32_t)k);
-    uint32_t per = 0, pieces = 1, items;
-    if (lo >= piece) {
-        pieces = min(max_pieces, (lo + piece - 1u) / piece);
-        items = cnt * pieces;  // <= 2^32 for the sizes accepted (nhalos * max_pieces is checked on the host)
-    } else {
-        per = lo >= single ? 1u : min(32u, max(1u, piece / max(lo, 1u)));
-        items = (cnt + per - 1u) / per;
-    }
-    s_cnt[k] = cnt;
-    s_items[k] = items;
-    __syncthreads();
-    if (k == 0) {
-        uint32_t pos = 0, it = 0;
-        for (int j = 0; j < kBuckets; ++j) {
-            const uint32_t c = s_cnt[j], n = s_items[j];
-            s_cnt[j] = pos;
-            s_items[j] = it;
-            pos += c;
-            it += n;
-        }
-        ctl[0] = 0;
-        ctl[1] = it;
-    }
-    __syncthreads();
-    plan[k] = BucketPlan{s_cnt[k], cnt, per, pieces, s_items[k]};
-}
-
 template <int BIN, bool BIG>
 __global__ void __launch_bounds__(CT_THREADS, 8) k_shell_count_queue(CountParams p, QueueParams q) {
     extern __shared__ uint32_t smem[];
@@ -498,13 +444,9 @@ __global__ void __launch_bounds__(CT_THREADS, 8) k_shell_count_queue(CountParams
     const uint32_t nitems = q.ctl[1];
     int bk = 0;  // claims only grow, so each warp's bucket search moves forward
     for (;;) {
-        uint32_t g = 0;
-        if (lane == 0) g = atomicAdd(q.ctl, 1u);
-        g = __shfl_sync(0xffffffffu, g, 0);
-        if (g >= nitems) break;
-        while (bk + 1 < kBuckets && __ldg(&q.plan[bk + 1].item0) <= g) ++bk;
-        const BucketPlan bp = q.plan[bk];
-        const uint32_t r = g - bp.item0;
+        BucketPlan bp;
+        uint32_t r;
+        if (!claim_item(q, nitems, lane, &bk, &bp, &r)) break;
         if (bp.per == 0) {
             const uint32_t pos = bp.start + r / bp.pieces, part = r % bp.pieces;
             const float4 c = p.halos[q.ord[pos]];
@@ -524,18 +466,6 @@ __global__ void __launch_bounds__(CT_THREADS, 8) k_shell_count_queue(CountParams
         }
     }
 }
-
-struct KeyFromEst {
-    const uint32_t* __restrict__ key;
-    __device__ __forceinline__ uint32_t operator()(uint64_t i) const { return key[i]; }
-};
-struct PayIndex {
-    __device__ __forceinline__ uint4 operator()(uint64_t i) const { return make_uint4((uint32_t)i, 0u, 0u, 0u); }
-};
-struct SinkOrd {
-    uint32_t* __restrict__ ord;
-    __device__ __forceinline__ void operator()(uint32_t g, uint32_t, const uint4& v) const { ord[g] = v.x; }
-};
 
 template <int BIN, bool BIG>
 int launch_variant(sjcs_ctx* ctx, const CountParams& p, size_t smem, cudaStream_t s) {
@@ -571,11 +501,8 @@ int launch_queue(sjcs_ctx* ctx, const CountParams& p, const Schedule& sc, size_t
     SJCS_CUDA_TRY(cudaMemsetAsync(hist, 0, kBuckets * sizeof(uint32_t), s));
     k_estimate<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(p, key, hist);
     SJCS_LAUNCH_CHECK();
-    int rc = radix_sort_records(n, 8, KeyFromEst{key}, PayIndex{}, SinkOrd{ord}, nullptr, nullptr, nullptr, nullptr,
-                                rhist, s);
+    int rc = order_and_plan(n, key, hist, sc, ord, plan, ctl, rhist, s);
     if (rc) return rc;
-    k_plan_items<<<1, kBuckets, 0, s>>>(hist, sc.piece, sc.max_pieces, sc.single, plan, ctl);
-    SJCS_LAUNCH_CHECK();
     auto kern = k_shell_count_queue<BIN, BIG>;
     if (smem > 48 * 1024)
         SJCS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));

@@ -355,7 +355,6 @@ Schedule resolve(const sjcs_schedule& in) {
 
 // The schedule a count call uses (ctx->mu held).
 Schedule schedule_for(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx) {
-    if (idx->kind != SJCS_INDEX_GRID) return resolve(sjcs_schedule{SJCS_SCHED_STATIC, 0, 0, 0});
     sjcs_schedule sc = q->sched;
     if (sc.mode == SJCS_SCHED_AUTO) {
         auto it = ctx->tuned.find(shape_key(q, idx));
@@ -399,7 +398,7 @@ int capture_step_body(sjcs_ctx* ctx, sjcs_query* q, const float* host_xyz, uint6
     SJCS_CUDA_TRY(cudaStreamWaitEvent(sc, join1, 0));
     const Schedule sched = schedule_for(ctx, q, idx);
     rc = idx->kind == SJCS_INDEX_GRID ? launch_shell_count(ctx, q, idx, sc, &sched)
-                                      : launch_morton_count(ctx, q, idx, sc);
+                                      : launch_morton_count(ctx, q, idx, sc, &sched);
     if (idx->pts) SJCS_CUDA_TRY(cudaFreeAsync(idx->pts, sc));
     if (idx->cell_start) SJCS_CUDA_TRY(cudaFreeAsync(idx->cell_start, sc));
     if (idx->leaves) SJCS_CUDA_TRY(cudaFreeAsync(idx->leaves, sc));
@@ -776,7 +775,7 @@ int sjcs_query_count(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx) {
     q->count_events.push_back(e1);
     cudaEventRecord(e0, s);
     const Schedule sc = schedule_for(ctx, q, idx);
-    rc = idx->kind == SJCS_INDEX_GRID ? launch_shell_count(ctx, q, idx, s, &sc) : launch_morton_count(ctx, q, idx, s);
+    rc = idx->kind == SJCS_INDEX_GRID ? launch_shell_count(ctx, q, idx, s, &sc) : launch_morton_count(ctx, q, idx, s, &sc);
     cudaEventRecord(e1, s);
     cudaEventRecord(q->ev_last, s);
     return rc;
@@ -941,10 +940,8 @@ int sjcs_autotune(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx, sjcs_sche
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(ctx->mu);
     std::vector<sjcs_schedule> cand{{SJCS_SCHED_STATIC, 0, 0, 0}};
-    if (idx->kind == SJCS_INDEX_GRID) {
-        for (uint32_t pc : {2048u, 8192u, 32768u, 131072u}) cand.push_back(sjcs_schedule{SJCS_SCHED_QUEUE, pc, 64u, 0});
-        cand.push_back(sjcs_schedule{SJCS_SCHED_QUEUE, 32768u, 256u, 0});
-    }
+    for (uint32_t pc : {2048u, 8192u, 32768u, 131072u}) cand.push_back(sjcs_schedule{SJCS_SCHED_QUEUE, pc, 64u, 0});
+    cand.push_back(sjcs_schedule{SJCS_SCHED_QUEUE, 32768u, 256u, 0});
     std::vector<float> ms(cand.size(), 0.0f);
     cudaStream_t s = ctx->s_count;
     SJCS_CUDA_TRY(cudaStreamWaitEvent(s, idx->ev_ready, 0));
@@ -961,7 +958,7 @@ int sjcs_autotune(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx, sjcs_sche
         const Schedule sc = resolve(c);
         cudaEventRecord(e0, s);
         int r = idx->kind == SJCS_INDEX_GRID ? launch_shell_count(ctx, q, idx, s, &sc)
-                                             : launch_morton_count(ctx, q, idx, s);
+                                             : launch_morton_count(ctx, q, idx, s, &sc);
         cudaEventRecord(e1, s);
         if (r) return r;
         if (cudaEventSynchronize(e1) != cudaSuccess) return fail(SJCS_ERR_CUDA, "autotune trial failed");

@@ -190,8 +190,10 @@ int morton_auto_level(uint64_t n, float radius_hint);
 int build_morton_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, int level, bool learned, bool verify,
                        sjcs_index* idx, cudaStream_t s);
 
-// morton_count.cu
-int launch_morton_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s);
+// morton_count.cu (sc as for launch_shell_count)
+struct Schedule;
+int launch_morton_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s,
+                        const Schedule* sc = nullptr);
 
 // sjcs_abi.cu: query preparation on stream s (radius table, shell lookup,
 // zeroed accumulators, Morton-sorted halos) and schedule resolution

@@ -109,7 +109,7 @@ def test_schedule_arguments_are_validated(ctx):
     q.destroy()
 
 
-def test_autotune_on_morton_indexes_keeps_static(ctx):
+def test_autotune_on_morton_indexes(ctx):
     rng = np.random.default_rng(34)
     p = rng.uniform(0, 1000, size=(50000, 3)).astype(np.float32)
     h = rng.uniform(0, 1000, size=(2000, 3)).astype(np.float32)
@@ -118,9 +118,27 @@ def test_autotune_on_morton_indexes_keeps_static(ctx):
         idx = ctx.build_index(p, radius_hint=5.0, kind=kind)
         q = ctx.query(h, r2)
         res = ctx.autotune(q, idx)
-        assert len(res["trial_ms"]) == 1 and res["chosen"]["mode"] == nat.SCHED_STATIC
-        q.set_schedule(nat.SCHED_QUEUE)  # Morton forms count with the static schedule
+        assert len(res["trial_ms"]) == 6 and res["chosen"]["mode"] in (nat.SCHED_STATIC, nat.SCHED_QUEUE)
         q.count(idx)
         assert np.array_equal(q.read_counts(), oracle.count(p, h, r2))
         idx.destroy()
         q.destroy()
+
+
+@pytest.mark.parametrize("kind", [nat.INDEX_MORTON, nat.INDEX_LEARNED])
+@pytest.mark.parametrize("qs", QUEUES)
+def test_queue_on_morton_forms_matches_oracle(kind, qs, ctx):
+    p = nat.gen_clustered_particles(17, 200000)
+    h = nat.gen_clustered_halos(18, 3000)
+    rng = np.random.default_rng(19)
+    h["point"][:30] = rng.choice([0.0, 1000.0, 2.0, 998.0], size=(30, 3))
+    for r2, per in [(nat.radius_table(0.01, 20, 64), True), (nat.radius_table(0.001, 5, 40), False),
+                    (np.array([400.0, 100.0, 2500.0], np.float32), True)]:
+        q = ctx.query(h, r2, periodic=per)
+        q.set_schedule(nat.SCHED_QUEUE, **qs)
+        idx = ctx.build_index(p, radius_hint=10.0, kind=kind)
+        q.count(idx)
+        got = q.read_counts()
+        idx.destroy()
+        q.destroy()
+        assert np.array_equal(got, oracle.count(p, h, r2, periodic=per, brute=len(r2) < 10)), (kind, r2[:3])
