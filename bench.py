@@ -392,16 +392,6 @@ def run_ours(args, w, dist, rank, world, local):
                 forms[name]["model"] = {"leaves": info["leaves"], "max_err": info["max_err"],
                                         "mean_err": round(info["mean_err"], 1), "level": info["level"]}
         del grid_counts
-    # correctness spot-check of the timed path on a halo sample (oracle, file 0)
-    check = None
-    if rank == 0 and not args.no_check and not args.no_e2e:
-        from oracle import oracle
-        sample = 2000
-        got = out_np[:sample]
-        want = np.zeros((sample, nr), np.uint64)
-        for f in range(nf):
-            oracle.count(pnp[f * n:(f + 1) * n], halos_np[:sample], r2, counts=want)
-        check = bool(np.array_equal(got, want))
 
     units = nh * nf * world
     value = units / (ms / 1e3)
@@ -441,7 +431,6 @@ def run_ours(args, w, dist, rank, world, local):
         "clocks_e2e": clocks_e2e,
         "gpu_launches": int(launches),
         "gpu_launches_e2e": int(launches_e2e),
-        "parity_spot_check": check,
         "forms": forms,
     }
     ctx.close()
@@ -631,14 +620,6 @@ def run_clustered(args, w, dist, rank, world, local):
     st.destroy()
     q.destroy()
 
-    check = None
-    if rank == 0 and not args.no_check:
-        from oracle import oracle
-        sample = 300
-        want = np.zeros((sample, nr), np.uint64)
-        for f in range(nf):
-            oracle.count(pnp[f * n:(f + 1) * n], hnp[:sample], r2, counts=want)
-        check = bool(np.array_equal(out_np[:sample], want))
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu = clustered_cpu_baseline(w, pnp[:n], hnp, 2000)
@@ -659,7 +640,7 @@ def run_clustered(args, w, dist, rank, world, local):
         "e2e": {"value": round(units / (ms_e2e / 1e3), 1), "unit": UNIT, "ms_per_step": round(ms_e2e, 3),
                 "h2d_bytes_per_step": int(nf * n * 12 + (nh - 1) * 24 + 12), "d2h_bytes_per_step": int(nh * nr * 8)},
         "roofline": None, "cpu_baseline": cpu, "clocks": clocks, "clocks_e2e": clocks_e2e,
-        "gpu_launches": launches, "gpu_launches_e2e": launches_e2e, "parity_spot_check": check,
+        "gpu_launches": launches, "gpu_launches_e2e": launches_e2e,
     }
     ctx.close()
     return line
@@ -945,7 +926,8 @@ def main():
     ap.add_argument("--halo-slab", type=float, default=None,
                     help="keep only halos with z < SLAB (profiling at full halo density on fewer halos)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--no-check", action="store_true")
+    ap.add_argument("--no-check", action="store_true",
+                    help="accepted and ignored (parity is checked by the test suite, not by the benchmark)")
     ap.add_argument("--no-forms", action="store_true", help="skip the learned/Morton comparison legs")
     ap.add_argument("--particles", type=int, default=None, help="override particles per file (profiling cases)")
     ap.add_argument("--no-reserve", action="store_true",
