@@ -167,6 +167,14 @@ int sjcs_ctx_memory(sjcs_ctx *ctx, uint64_t *free_bytes, uint64_t *pool_bytes);
 int sjcs_ctx_stream(const sjcs_ctx *ctx, int which, void **stream);
 /* Number of kernels this library has launched in this process so far. */
 uint64_t sjcs_launch_counter(void);
+/* Whether an index build's kernels may run beside the counts already queued
+ * on the context (overlap != 0), or wait for them (overlap == 0, the
+ * default).  Either way the build's host-to-device copy overlaps the counts.
+ * On one GPU the two kinds of kernel compete for the same SMs and L2, so
+ * running them back to back is faster than side by side; the reference's
+ * backlog pipeline (src/astr_rcount/main.c:266-350) overlaps them because its
+ * builds and searches use separate CPU threads. */
+int sjcs_ctx_set_overlap(sjcs_ctx *ctx, int overlap);
 
 /* ---- pinned host memory (for the driver's file reads) -------------------- */
 

@@ -95,6 +95,7 @@ _SIGS = {
     "sjcs_ctx_trim": (_c.c_int, [_vp]),
     "sjcs_ctx_memory": (_c.c_int, [_vp, _c.POINTER(_u64), _c.POINTER(_u64)]),
     "sjcs_launch_counter": (_c.c_uint64, []),
+    "sjcs_ctx_set_overlap": (_c.c_int, [_vp, _c.c_int]),
     "sjcs_host_alloc": (_c.c_int, [_c.c_size_t, _pp]),
     "sjcs_host_free": (_c.c_int, [_vp]),
     "sjcs_index_build": (_c.c_int, [_vp, _vp, _u64, _c.POINTER(sjcs_index_opts), _pp]),
@@ -327,6 +328,10 @@ class Context:
         """A file step (copy, build, count) captured as a CUDA graph over a pinned
         host buffer of n particles (Step.buffer, an (n, 3) float32 array)."""
         return Step(self, query, n, _make_opts(radius_hint, None, kind, level, verify))
+
+    def set_overlap(self, overlap: bool) -> None:
+        """Let index builds' kernels run beside queued counts (default: they wait)."""
+        _check(lib().sjcs_ctx_set_overlap(self._h, 1 if overlap else 0))
 
     def autotune(self, query: "Query", index: "Index") -> "dict":
         """Time the candidate count schedules on the full query; keep the fastest."""

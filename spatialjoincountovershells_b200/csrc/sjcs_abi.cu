@@ -244,6 +244,14 @@ void free_index(sjcs_index* idx) {
     delete idx;
 }
 
+// Unless builds may overlap counts: the build kernels queued next on s wait
+// for every count queued so far (the copies queued before them do not).
+void order_after_counts(sjcs_ctx* ctx, cudaStream_t s) {
+    if (ctx->overlap || !ctx->ev_counts) return;
+    if (cudaEventRecord(ctx->ev_counts, ctx->s_count) == cudaSuccess) cudaStreamWaitEvent(s, ctx->ev_counts, 0);
+    cudaGetLastError();
+}
+
 // Validated copy of the build options.
 int check_opts(const sjcs_index_opts* opts, sjcs_index_opts* o_out) {
     sjcs_index_opts o{};
@@ -315,6 +323,7 @@ int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, c
         idx->had_h2d = true;
     }
     cudaEventRecord(idx->ev_h2d, s);
+    order_after_counts(ctx, s);
     rc = enqueue_build(ctx, idx, d_xyz, n, o, s);
     if (rc) {
         free_index(idx);
@@ -443,6 +452,7 @@ int sjcs_ctx_create(int device, sjcs_ctx** out) {
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     SJCS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->s_build, cudaStreamNonBlocking));
     SJCS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->s_count, cudaStreamNonBlocking));
+    SJCS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_counts, cudaEventDisableTiming));
     // Keep freed stream-ordered memory cached in the pool: every file's index
     // and scratch reuse the previous file's pages without new cudaMalloc calls.
     cudaMemPool_t pool;
@@ -462,6 +472,7 @@ int sjcs_ctx_destroy(sjcs_ctx* ctx) {
     cudaStreamSynchronize(ctx->s_count);
     cudaStreamDestroy(ctx->s_build);
     cudaStreamDestroy(ctx->s_count);
+    if (ctx->ev_counts) cudaEventDestroy(ctx->ev_counts);
     ctx->magic = 0;
     delete ctx;
     return SJCS_OK;
@@ -479,6 +490,13 @@ int sjcs_ctx_sync(sjcs_ctx* ctx) {
 int sjcs_ctx_stream(const sjcs_ctx* ctx, int which, void** stream) {
     if (!valid_ctx(ctx) || !stream || (which != 0 && which != 1)) return fail(SJCS_ERR_INVALID, "invalid argument");
     *stream = (void*)(which == 0 ? ctx->s_build : ctx->s_count);
+    return SJCS_OK;
+}
+
+int sjcs_ctx_set_overlap(sjcs_ctx* ctx, int overlap) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    ctx->overlap = overlap != 0;
     return SJCS_OK;
 }
 
@@ -608,6 +626,7 @@ int sjcs_index_build_compressed(sjcs_ctx* ctx, const uint16_t* uv, uint64_t n, c
         idx->had_h2d = true;
     }
     cudaEventRecord(idx->ev_h2d, s);
+    order_after_counts(ctx, s);
     rc = launch_decode(d_uv, n, g, d_xyz, s);
     if (!rc) rc = enqueue_build(ctx, idx, d_xyz, n, o, s);
     if (rc) {

@@ -121,6 +121,8 @@ struct sjcs_ctx {
     cudaStream_t s_count;  // halo upload/sort, shell counts, count read-back
     std::mutex mu;
     std::map<std::string, sjcs_schedule> tuned;  // autotuned schedules by workload shape
+    bool overlap = false;    // builds' kernels may run beside queued counts
+    cudaEvent_t ev_counts = nullptr;  // marks the counts queued so far (build ordering)
 };
 
 namespace sjcs {
