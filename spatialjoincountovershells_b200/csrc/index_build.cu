@@ -9,7 +9,8 @@
 // -- so any index that returns a superset of the in-box points gives the same
 // counts.  Here the index is a uniform cell grid:
 //   pass 0   key = cell of (x,y,z) and payload = (x,y,z), read from the AoS input
-//   passes   stable LSD radix sort of (key, payload), 8 bits per pass
+//   passes   stable LSD radix sort of (key, payload), 8 bits per pass (9 for
+//            25-27-bit cell keys: three passes instead of four)
 //   last     writes the sorted particles as float4 and the sorted keys
 //   offsets  cell_start[c] = first sorted slot of cell c (boundary fill)
 #include <algorithm>
@@ -94,19 +95,20 @@ GridGeom auto_grid(uint64_t n, float radius_hint, const uint32_t* grid_req) {
     } else {
         // Rows of cells run along x and are looked up with two offsets, so x
         // can be finer than y/z for free: cells are 2.5x longer in y and z.
-        // Target about 1.6 cells per particle, at most 2^28 cells, and keep
-        // y/z cells >= R/2 so a query box spans at most ~5x5 rows.
-        const double target = std::min(std::max(1.6 * (double)n, 4096.0), 268435456.0);
+        // Target about 1.6 cells per particle, at most 2^27 cells (a 27-bit
+        // cell key sorts in three 9-bit radix passes), and keep y/z cells
+        // >= R/2 so a query box spans at most 5x5 rows.
+        constexpr double kMaxCells = 134217728.0;  // 2^27
+        const double target = std::min(std::max(1.6 * (double)n, 4096.0), kMaxCells);
         double hyz = std::cbrt(2.5e9 / target);
         if (radius_hint > 0.0f) hyz = std::max(hyz, 0.5 * (double)radius_hint);
-        const double hx = hyz / 2.5;
-        G[0] = (int)std::min(std::max(std::ceil(1000.0 / hx), 1.0), 4096.0);
-        G[1] = (int)std::min(std::max(std::ceil(1000.0 / hyz), 1.0), 4096.0);
-        G[2] = G[1];
-        while ((uint64_t)G[0] * G[1] * G[2] > 268435456ull) {
-            G[0] = std::max(1, G[0] * 7 / 8);
-            G[1] = std::max(1, G[1] * 7 / 8);
+        for (;;) {
+            const double hx = hyz / 2.5;
+            G[0] = (int)std::min(std::max(std::ceil(1000.0 / hx), 1.0), 4096.0);
+            G[1] = (int)std::min(std::max(std::ceil(1000.0 / hyz), 1.0), 4096.0);
             G[2] = G[1];
+            if ((double)G[0] * G[1] * G[2] <= kMaxCells) break;
+            hyz *= 1.01;  // rounding up per axis overshot the cap
         }
     }
     for (int a = 0; a < 3; ++a) {
@@ -123,11 +125,19 @@ int grid_key_bits(const GridGeom& g) {
     return key_bits;
 }
 
+int grid_digit_bits(const GridGeom& g) {
+    const int kb = grid_key_bits(g);
+    return (kb > 24 && kb <= 27) ? 9 : 8;  // three passes instead of four
+}
+
 int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, cudaStream_t s) {
     static_assert(sizeof(Gap) == 12, "gap records are 12 bytes");
-    int rc = radix_sort_records(n, grid_key_bits(g), KeysFromParticles{d_xyz, g}, PayFromParticles{d_xyz},
-                                SinkParticles{b.kfinal, reinterpret_cast<uint4*>(b.pts)}, b.kx, b.px, b.ky, b.py,
-                                b.hist, s, b.partials);
+    const SinkParticles sink{b.kfinal, reinterpret_cast<uint4*>(b.pts)};
+    int rc = b.digit_bits == 9
+                 ? radix_sort_records<9>(n, grid_key_bits(g), KeysFromParticles{d_xyz, g}, PayFromParticles{d_xyz},
+                                         sink, b.kx, b.px, b.ky, b.py, b.hist, s, b.partials)
+                 : radix_sort_records<8>(n, grid_key_bits(g), KeysFromParticles{d_xyz, g}, PayFromParticles{d_xyz},
+                                         sink, b.kx, b.px, b.ky, b.py, b.hist, s, b.partials);
     if (rc) return rc;
     return fill_cell_table(b.kfinal, n, g.ncells, b.cell_start, b.gaps, b.ngaps, s);
 }
@@ -157,7 +167,8 @@ int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGe
     b.pts = idx->pts;
     b.cell_start = idx->cell_start;
     const uint64_t ntiles = (n + RS_TILE - 1) / RS_TILE;
-    const int passes = (grid_key_bits(g) + RS_BITS - 1) / RS_BITS;
+    b.digit_bits = grid_digit_bits(g);
+    const int passes = (grid_key_bits(g) + b.digit_bits - 1) / b.digit_bits;
     StreamScratch scr(s);  // freed (stream-ordered) on every return path
     SJCS_CUDA_TRY(scr.alloc(&b.kfinal, nalloc * sizeof(uint32_t)));
     if (passes > 1) {
@@ -168,7 +179,7 @@ int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGe
         SJCS_CUDA_TRY(scr.alloc(&b.ky, nalloc * sizeof(uint32_t)));
         SJCS_CUDA_TRY(scr.alloc(&b.py, nalloc * sizeof(uint4)));
     }
-    SJCS_CUDA_TRY(scr.alloc(&b.hist, ((uint64_t)RS_BINS * (ntiles ? ntiles : 1)) * sizeof(uint32_t)));
+    SJCS_CUDA_TRY(scr.alloc(&b.hist, ((uint64_t)(1u << b.digit_bits) * (ntiles ? ntiles : 1)) * sizeof(uint32_t)));
     SJCS_CUDA_TRY(scr.alloc(&b.gaps, kGridGaps * sizeof(Gap)));
     SJCS_CUDA_TRY(scr.alloc(&b.ngaps, sizeof(uint32_t)));
     return build_grid_into(d_xyz, n, g, b, s);

@@ -1,5 +1,5 @@
-// Stable LSD radix sort of (u32 key, 16-byte payload) records, 8-bit digits,
-// reduce-then-scan per digit pass:
+// Stable LSD radix sort of (u32 key, 16-byte payload) records, 8- or 9-bit
+// digits, reduce-then-scan per digit pass:
 //   k_radix_upsweep    per-tile digit histogram           -> hist[digit][tile]
 //   exclusive_scan_u32 over hist (digit-major)            -> global slot base of (digit, tile)
 //   k_radix_downsweep  stable in-tile rank (warp match),   shared-memory exchange of key and
@@ -19,6 +19,7 @@
 
 #include <cuda_runtime.h>
 #include <cstdint>
+#include <type_traits>
 
 #include "sjcs_internal.cuh"
 
@@ -28,12 +29,22 @@ constexpr int RS_THREADS = 512;
 constexpr int RS_ITEMS = 8;
 constexpr int RS_TILE = RS_THREADS * RS_ITEMS;  // 4096 records per tile
 constexpr int RS_WARPS = RS_THREADS / 32;
-constexpr int RS_BITS = 8;
+constexpr int RS_BITS = 8;  // default digit width
 constexpr int RS_BINS = 1 << RS_BITS;
 constexpr int RS_SUBHIST = 4;  // upsweep: warps share RS_SUBHIST histograms
 // dynamic shared memory of the downsweep: exchanged keys + payloads, and for
 // array payloads the source slot of every ranked record
 constexpr size_t RS_DOWN_SMEM = (size_t)RS_TILE * (sizeof(uint32_t) + sizeof(uint4) + sizeof(uint16_t));
+
+// A digit of BITS bits (8 or 9).  The downsweep keeps one counter per warp
+// and bin; a tile holds 4096 records, so 16-bit counters suffice and keep the
+// 9-bit downsweep's shared memory at two blocks per SM.
+template <int BITS>
+struct RsDigit {
+    static_assert(BITS == 8 || BITS == 9, "digits of 8 or 9 bits");
+    static constexpr int BINS = 1 << BITS;
+    using Cnt = typename std::conditional<(BITS > 8), uint16_t, uint32_t>::type;
+};
 
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
@@ -59,22 +70,23 @@ struct SinkRecords {
     }
 };
 
-template <class KeyOp>
+template <int BITS, class KeyOp>
 __global__ void __launch_bounds__(RS_THREADS)
 k_radix_upsweep(KeyOp kop, uint64_t n, int shift, uint32_t* __restrict__ hist, uint32_t ntiles) {
-    __shared__ uint32_t sh[RS_SUBHIST][RS_BINS];
+    constexpr int BINS = RsDigit<BITS>::BINS;
+    __shared__ uint32_t sh[RS_SUBHIST][BINS];
     const int tid = threadIdx.x;
-    for (int i = tid; i < RS_SUBHIST * RS_BINS; i += RS_THREADS) (&sh[0][0])[i] = 0;
+    for (int i = tid; i < RS_SUBHIST * BINS; i += RS_THREADS) (&sh[0][0])[i] = 0;
     __syncthreads();
     const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
     uint32_t* mine = sh[(tid >> 5) % RS_SUBHIST];
 #pragma unroll
     for (int i = 0; i < RS_ITEMS; ++i) {
         const uint64_t idx = base + (uint64_t)i * RS_THREADS + tid;
-        if (idx < n) atomicAdd(&mine[(kop(idx) >> shift) & (RS_BINS - 1)], 1u);
+        if (idx < n) atomicAdd(&mine[(kop(idx) >> shift) & (BINS - 1)], 1u);
     }
     __syncthreads();
-    for (int d = tid; d < RS_BINS; d += RS_THREADS) {
+    for (int d = tid; d < BINS; d += RS_THREADS) {
         uint32_t s = 0;
 #pragma unroll
         for (int h = 0; h < RS_SUBHIST; ++h) s += sh[h][d];
@@ -101,7 +113,7 @@ struct PayIsArray<PayFromArray> {
     static constexpr bool value = true;
 };
 
-template <class KeyOp, class PayOp, class Sink>
+template <int BITS, class KeyOp, class PayOp, class Sink>
 __global__ void __launch_bounds__(RS_THREADS)
 k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
                   const uint32_t* __restrict__ offs, uint32_t ntiles, Sink sink) {
@@ -110,7 +122,10 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
     // ranked records then carry their source slot.  Computed payloads are
     // produced at the scatter, in rank order.
     constexpr bool kAsync = PayIsArray<PayOp>::value;
-    __shared__ uint32_t warp_cnt[RS_WARPS][RS_BINS];
+    constexpr int RS_BINS = RsDigit<BITS>::BINS;  // bins of this pass's digit
+    static_assert(RS_BINS <= RS_THREADS, "one thread per bin in the digit scan");
+    using Cnt = typename RsDigit<BITS>::Cnt;
+    __shared__ Cnt warp_cnt[RS_WARPS][RS_BINS];
     __shared__ uint32_t dstart[RS_BINS];
     __shared__ uint32_t gbase[RS_BINS];
     __shared__ uint32_t wsum[RS_BINS / 32];
@@ -152,7 +167,7 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
         const uint32_t before = __popc(peers & lt);
         const uint32_t c = valid ? warp_cnt[warp][d] : 0u;
         __syncwarp();
-        if (valid && before == 0) warp_cnt[warp][d] = c + __popc(peers);
+        if (valid && before == 0) warp_cnt[warp][d] = (Cnt)(c + __popc(peers));
         __syncwarp();
         key[i] = k;
         pos[i] = valid ? c + before : 0xffffffffu;
@@ -166,7 +181,7 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
 #pragma unroll
         for (int w = 0; w < RS_WARPS; ++w) {
             const uint32_t t = warp_cnt[w][tid];
-            warp_cnt[w][tid] = tot;
+            warp_cnt[w][tid] = (Cnt)tot;
             tot += t;
         }
         incl = tot;
@@ -210,14 +225,14 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
     }
 }
 
-template <class KeyOp, class PayOp, class Sink>
+template <int BITS = RS_BITS, class KeyOp, class PayOp, class Sink>
 int radix_pass(KeyOp kop, PayOp pop, Sink sink, uint64_t n, int shift, uint32_t* hist, uint32_t ntiles,
                cudaStream_t s, uint32_t* partials) {
-    k_radix_upsweep<<<ntiles, RS_THREADS, 0, s>>>(kop, n, shift, hist, ntiles);
+    k_radix_upsweep<BITS><<<ntiles, RS_THREADS, 0, s>>>(kop, n, shift, hist, ntiles);
     SJCS_LAUNCH_CHECK();
-    int rc = exclusive_scan_u32(hist, (uint64_t)RS_BINS * ntiles, s, partials);
+    int rc = exclusive_scan_u32(hist, (uint64_t)RsDigit<BITS>::BINS * ntiles, s, partials);
     if (rc) return rc;
-    auto kern = k_radix_downsweep<KeyOp, PayOp, Sink>;
+    auto kern = k_radix_downsweep<BITS, KeyOp, PayOp, Sink>;
     SJCS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)RS_DOWN_SMEM));
     kern<<<ntiles, RS_THREADS, RS_DOWN_SMEM, s>>>(kop, pop, n, shift, hist, ntiles, sink);
     SJCS_LAUNCH_CHECK();
@@ -227,17 +242,18 @@ int radix_pass(KeyOp kop, PayOp pop, Sink sink, uint64_t n, int shift, uint32_t*
 // Sort n records by their low key_bits key bits.  Pass 0 reads (kop0, pop0);
 // the last pass hands every record to `final`; passes in between ping-pong
 // through (keys_x, pay_x) and (keys_y, pay_y), arranged so that the pass
-// before the last one writes the x buffers.  hist holds RS_BINS * ntiles u32;
-// partials (optional) holds the scan's scan_partials_needed(RS_BINS * ntiles).
-template <class KeyOp0, class PayOp0, class FinalSink>
+// before the last one writes the x buffers.  BITS is the digit width (8 or
+// 9): hist holds RsDigit<BITS>::BINS * ntiles u32 and partials (optional)
+// holds the scan's scan_partials_needed(RsDigit<BITS>::BINS * ntiles).
+template <int BITS = RS_BITS, class KeyOp0, class PayOp0, class FinalSink>
 int radix_sort_records(uint64_t n, int key_bits, KeyOp0 kop0, PayOp0 pop0, FinalSink final_sink,
                        uint32_t* keys_x, uint4* pay_x, uint32_t* keys_y, uint4* pay_y, uint32_t* hist,
                        cudaStream_t s, uint32_t* partials = nullptr) {
     if (n == 0) return SJCS_OK;
     const uint32_t ntiles = (uint32_t)((n + RS_TILE - 1) / RS_TILE);
-    const int passes = key_bits <= 0 ? 1 : (key_bits + RS_BITS - 1) / RS_BITS;
+    const int passes = key_bits <= 0 ? 1 : (key_bits + BITS - 1) / BITS;
     for (int p = 0; p < passes; ++p) {
-        const int shift = p * RS_BITS;
+        const int shift = p * BITS;
         const bool first = (p == 0), last = (p == passes - 1);
         // record buffers written by pass p (p < passes-1): x when (passes-2-p) is even
         const bool to_x = ((passes - 2 - p) % 2) == 0;
@@ -247,14 +263,14 @@ int radix_sort_records(uint64_t n, int key_bits, KeyOp0 kop0, PayOp0 pop0, Final
         uint4* vin = to_x ? pay_y : pay_x;
         int rc;
         if (first && last)
-            rc = radix_pass(kop0, pop0, final_sink, n, shift, hist, ntiles, s, partials);
+            rc = radix_pass<BITS>(kop0, pop0, final_sink, n, shift, hist, ntiles, s, partials);
         else if (first)
-            rc = radix_pass(kop0, pop0, SinkRecords{kout, vout}, n, shift, hist, ntiles, s, partials);
+            rc = radix_pass<BITS>(kop0, pop0, SinkRecords{kout, vout}, n, shift, hist, ntiles, s, partials);
         else if (last)
-            rc = radix_pass(KeysFromArray{keys_x}, PayFromArray{pay_x}, final_sink, n, shift, hist, ntiles, s,
+            rc = radix_pass<BITS>(KeysFromArray{keys_x}, PayFromArray{pay_x}, final_sink, n, shift, hist, ntiles, s,
                             partials);
         else
-            rc = radix_pass(KeysFromArray{kin}, PayFromArray{vin}, SinkRecords{kout, vout}, n, shift, hist, ntiles,
+            rc = radix_pass<BITS>(KeysFromArray{kin}, PayFromArray{vin}, SinkRecords{kout, vout}, n, shift, hist, ntiles,
                             s, partials);
         if (rc) return rc;
     }

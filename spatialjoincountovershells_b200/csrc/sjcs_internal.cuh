@@ -242,17 +242,19 @@ struct GridBuildBuffers {
     float4* pts;          // n sorted particles (output)
     uint32_t* cell_start; // ncells + 1 (output)
     uint32_t* kfinal;     // n
-    uint32_t* kx;         // n (needed when the key has more than 8 bits)
+    uint32_t* kx;         // n (needed for two or more passes)
     uint4* px;            // n
-    uint32_t* ky;         // n (needed when the key has more than 16 bits)
+    uint32_t* ky;         // n (needed for three or more passes)
     uint4* py;            // n
-    uint32_t* hist;       // 256 * ceil(n / 4096)
-    uint32_t* partials;   // scan_partials_needed(256 * ceil(n / 4096))
+    uint32_t* hist;       // 2^digit_bits * ceil(n / 4096)
+    uint32_t* partials;   // scan_partials_needed(2^digit_bits * ceil(n / 4096)), or null
     void* gaps;           // kGridGaps gap records (12 bytes each)
     uint32_t* ngaps;      // 1
+    int digit_bits;       // radix digit: 9, or 8 (also for 0)
 };
 constexpr uint32_t kGridGaps = 1u << 16;
 int grid_key_bits(const GridGeom& g);
+int grid_digit_bits(const GridGeom& g);  // 9 for 25-27-bit cell keys, else 8
 int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, cudaStream_t s);
 // cell_start[c] = first slot of cell c, from the cell ids of the sorted particles.
 int fill_cell_table(const uint32_t* sorted_cells, uint64_t n, uint64_t ncells, uint32_t* cell_start, void* gaps,
