@@ -122,23 +122,34 @@ class ClockSampler:
         self.proc = None
         self.lines: list[str] = []
         self.thread = None
+        self.first = threading.Event()
 
     def __enter__(self):
         exe = shutil.which("nvidia-smi")
         if exe:
             self.proc = subprocess.Popen([exe, f"--id={self.device}", f"--query-gpu={self.FIELDS}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
                                          stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.thread = threading.Thread(target=self._pump, daemon=True)
             self.thread.start()
+            # nvidia-smi takes a moment to start: the timed region begins only
+            # once it is sampling, so even a short region has samples around it
+            self.first.wait(timeout=10)
+            self.n_enter = len(self.lines)
         return self
 
     def _pump(self):
         for ln in self.proc.stdout:
             self.lines.append(ln.strip())
+            self.first.set()
 
     def __exit__(self, *exc):
         if self.proc:
+            # a region shorter than the sampling period: take the sample that
+            # follows it too (the GPU is still at its loaded clocks)
+            t_end = time.time() + 1.0
+            while len(self.lines) <= getattr(self, "n_enter", 0) and time.time() < t_end:
+                time.sleep(0.02)
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
@@ -920,7 +931,7 @@ def run_reference_arm(args, w):
 def main():
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--small", action="store_true", help="a 50x smaller workload (smoke runs, CPU tests)")

@@ -9,6 +9,7 @@
 // -- so any index that returns a superset of the in-box points gives the same
 // counts.  Here the index is a uniform cell grid:
 //   pass 0   key = cell of (x,y,z) and payload = (x,y,z), read from the AoS input
+//            (staged in shared memory a tile at a time when 16-byte aligned)
 //   passes   stable LSD radix sort of (key, payload), 8 bits per pass (9 for
 //            25-27-bit cell keys: three passes instead of four)
 //   last     writes the sorted particles as float4 and the sorted keys
@@ -25,8 +26,9 @@ namespace {
 struct KeysFromParticles {
     const float* __restrict__ xyz;
     GridGeom g;
+    __device__ __forceinline__ uint32_t key_of(float x, float y, float z) const { return cell_key(g, x, y, z); }
     __device__ __forceinline__ uint32_t operator()(uint64_t i) const {
-        return cell_key(g, xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        return key_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
     }
 };
 struct PayFromParticles {
@@ -130,14 +132,26 @@ int grid_digit_bits(const GridGeom& g) {
     return (kb > 24 && kb <= 27) ? 9 : 8;  // three passes instead of four
 }
 
+template <int BITS, class PayOp0>
+int sort_particles(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, PayOp0 pop0,
+                   cudaStream_t s) {
+    return radix_sort_records<BITS>(n, grid_key_bits(g), KeysFromParticles{d_xyz, g}, pop0,
+                                    SinkParticles{b.kfinal, reinterpret_cast<uint4*>(b.pts)}, b.kx, b.px, b.ky,
+                                    b.py, b.hist, s, b.partials);
+}
+
 int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, cudaStream_t s) {
     static_assert(sizeof(Gap) == 12, "gap records are 12 bytes");
-    const SinkParticles sink{b.kfinal, reinterpret_cast<uint4*>(b.pts)};
-    int rc = b.digit_bits == 9
-                 ? radix_sort_records<9>(n, grid_key_bits(g), KeysFromParticles{d_xyz, g}, PayFromParticles{d_xyz},
-                                         sink, b.kx, b.px, b.ky, b.py, b.hist, s, b.partials)
-                 : radix_sort_records<8>(n, grid_key_bits(g), KeysFromParticles{d_xyz, g}, PayFromParticles{d_xyz},
-                                         sink, b.kx, b.px, b.ky, b.py, b.hist, s, b.partials);
+    // A 16-byte-aligned particle array is staged tile by tile in the first
+    // pass; any other alignment is read particle by particle.
+    const bool staged = (reinterpret_cast<uintptr_t>(d_xyz) & 15u) == 0;
+    int rc;
+    if (b.digit_bits == 9)
+        rc = staged ? sort_particles<9>(d_xyz, n, g, b, PayFromXyzStaged{d_xyz}, s)
+                    : sort_particles<9>(d_xyz, n, g, b, PayFromParticles{d_xyz}, s);
+    else
+        rc = staged ? sort_particles<8>(d_xyz, n, g, b, PayFromXyzStaged{d_xyz}, s)
+                    : sort_particles<8>(d_xyz, n, g, b, PayFromParticles{d_xyz}, s);
     if (rc) return rc;
     return fill_cell_table(b.kfinal, n, g.ncells, b.cell_start, b.gaps, b.ngaps, s);
 }

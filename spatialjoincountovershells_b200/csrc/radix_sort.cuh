@@ -113,6 +113,26 @@ struct PayIsArray<PayFromArray> {
     static constexpr bool value = true;
 };
 
+// Payload of a first pass over a 16-byte-aligned array of (x, y, z) floats:
+// the downsweep stages each tile's 48 KB of particles in shared memory with
+// cp.async, then takes the keys (KeyOp::key_of(x, y, z)) and the payloads
+// (x, y, z, 0) from there instead of reading each particle twice.
+struct PayFromXyzStaged {
+    const float* __restrict__ xyz;
+    __device__ __forceinline__ uint4 operator()(uint64_t i) const {
+        return make_uint4(__float_as_uint(xyz[3 * i]), __float_as_uint(xyz[3 * i + 1]),
+                          __float_as_uint(xyz[3 * i + 2]), 0u);
+    }
+};
+template <class PayOp>
+struct PayIsXyz {
+    static constexpr bool value = false;
+};
+template <>
+struct PayIsXyz<PayFromXyzStaged> {
+    static constexpr bool value = true;
+};
+
 template <int BITS, class KeyOp, class PayOp, class Sink>
 __global__ void __launch_bounds__(RS_THREADS)
 k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
@@ -122,6 +142,7 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
     // ranked records then carry their source slot.  Computed payloads are
     // produced at the scatter, in rank order.
     constexpr bool kAsync = PayIsArray<PayOp>::value;
+    constexpr bool kXyz = PayIsXyz<PayOp>::value;  // particles staged in xpay
     constexpr int RS_BINS = RsDigit<BITS>::BINS;  // bins of this pass's digit
     static_assert(RS_BINS <= RS_THREADS, "one thread per bin in the digit scan");
     using Cnt = typename RsDigit<BITS>::Cnt;
@@ -132,7 +153,8 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
     extern __shared__ uint4 xdyn[];
     uint4* xpay = xdyn;                                            // [RS_TILE]: rank order, or load order (kAsync)
     uint32_t* xkey = reinterpret_cast<uint32_t*>(xdyn + RS_TILE);  // [RS_TILE], rank order
-    uint16_t* xsrc = reinterpret_cast<uint16_t*>(xkey + RS_TILE);  // [RS_TILE], rank order (kAsync)
+    uint16_t* xsrc = reinterpret_cast<uint16_t*>(xkey + RS_TILE);  // [RS_TILE], rank order (kAsync, kXyz)
+    const float* sxyz = reinterpret_cast<const float*>(xdyn);      // [3 * RS_TILE] in load order (kXyz)
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const uint32_t tile = blockIdx.x;
@@ -140,6 +162,9 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
     const uint64_t rem = n - tile_base;
     const uint32_t tile_n = rem < (uint64_t)RS_TILE ? (uint32_t)rem : (uint32_t)RS_TILE;
     const uint32_t wbase = (uint32_t)warp * 32u * RS_ITEMS;
+    // The tile's global digit bases are needed only after the ranking: load
+    // them now so their latency overlaps it.
+    const uint32_t my_gbase = tid < RS_BINS ? offs[(uint64_t)tid * ntiles + tile] : 0u;
 
     if constexpr (kAsync) {
 #pragma unroll
@@ -151,17 +176,38 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
 
     for (int d = lane; d < RS_BINS; d += 32) warp_cnt[warp][d] = 0;
     __syncwarp();
+    if constexpr (kXyz) {
+        // tile_base * 12 bytes is a multiple of 16; a ragged last tile ends
+        // with up to three 4-byte words loaded plainly
+        const uint32_t words = tile_n * 3u, chunks = words >> 2;
+        const float* src = pop.xyz + 3 * tile_base;
+        float* dst = reinterpret_cast<float*>(xdyn);
+        for (uint32_t c = (uint32_t)tid; c < chunks; c += RS_THREADS) cp_async16(dst + 4 * c, src + 4 * c);
+        for (uint32_t w = chunks * 4u + (uint32_t)tid; w < words; w += RS_THREADS) dst[w] = src[w];
+        cp_async_wait_all();
+        __syncthreads();
+    }
 
     // Warp w owns tile slots [w*32*ITEMS, (w+1)*32*ITEMS); item i of lane l is
     // slot w*32*ITEMS + i*32 + l, so loads are coalesced and the stable order
     // inside the warp is item-major, lane-minor.
+    // All keys are loaded first, so their loads are in flight together; the
+    // ranking that follows is a dependent chain through the warp's counters.
     uint32_t key[RS_ITEMS], pos[RS_ITEMS];
+#pragma unroll
+    for (int i = 0; i < RS_ITEMS; ++i) {
+        const uint32_t loc = wbase + (uint32_t)i * 32u + (uint32_t)lane;
+        if constexpr (kXyz)
+            key[i] = loc < tile_n ? kop.key_of(sxyz[3 * loc], sxyz[3 * loc + 1], sxyz[3 * loc + 2]) : 0u;
+        else
+            key[i] = loc < tile_n ? kop(tile_base + loc) : 0u;
+    }
     const uint32_t lt = lanemask_lt();
 #pragma unroll
     for (int i = 0; i < RS_ITEMS; ++i) {
         const uint32_t loc = wbase + (uint32_t)i * 32u + (uint32_t)lane;
         const bool valid = loc < tile_n;
-        const uint32_t k = valid ? kop(tile_base + loc) : 0u;
+        const uint32_t k = key[i];
         const uint32_t d = valid ? ((k >> shift) & (RS_BINS - 1)) : (uint32_t)RS_BINS;
         const uint32_t peers = __match_any_sync(0xffffffffu, d);
         const uint32_t before = __popc(peers & lt);
@@ -169,7 +215,6 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
         __syncwarp();
         if (valid && before == 0) warp_cnt[warp][d] = (Cnt)(c + __popc(peers));
         __syncwarp();
-        key[i] = k;
         pos[i] = valid ? c + before : 0xffffffffu;
     }
     __syncthreads();
@@ -197,7 +242,7 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
         uint32_t add = 0;
         for (int w = 0; w < warp; ++w) add += wsum[w];
         dstart[tid] = incl - tot + add;
-        gbase[tid] = offs[(uint64_t)tid * ntiles + tile];
+        gbase[tid] = my_gbase;
     }
     __syncthreads();
 
@@ -208,7 +253,7 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
             pos[i] += dstart[d] + warp_cnt[warp][d];
             const uint32_t loc = wbase + (uint32_t)i * 32u + (uint32_t)lane;
             xkey[pos[i]] = key[i];
-            if constexpr (kAsync) xsrc[pos[i]] = (uint16_t)loc;
+            if constexpr (kAsync || kXyz) xsrc[pos[i]] = (uint16_t)loc;
             else xpay[pos[i]] = pop(tile_base + loc);
         }
     }
@@ -220,7 +265,15 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
         if (j < tile_n) {
             const uint32_t kk = xkey[j];
             const uint32_t d = (kk >> shift) & (RS_BINS - 1);
-            sink(gbase[d] + (j - dstart[d]), kk, kAsync ? xpay[xsrc[j]] : xpay[j]);
+            uint4 v;
+            if constexpr (kXyz) {
+                const uint32_t src = xsrc[j];
+                v = make_uint4(__float_as_uint(sxyz[3 * src]), __float_as_uint(sxyz[3 * src + 1]),
+                               __float_as_uint(sxyz[3 * src + 2]), 0u);
+            } else {
+                v = kAsync ? xpay[xsrc[j]] : xpay[j];
+            }
+            sink(gbase[d] + (j - dstart[d]), kk, v);
         }
     }
 }

@@ -221,6 +221,34 @@ def test_device_pointer_api(ctx):
     assert np.array_equal(got, oracle.count(p, h, r2))
 
 
+@pytest.mark.parametrize("offset", [0, 1, 2, 3])
+def test_device_particles_at_any_alignment(offset, ctx):
+    # The first radix pass stages a 16-byte-aligned particle array in shared
+    # memory a tile at a time and reads any other one particle by particle:
+    # same counts at every float offset, with a ragged last tile whose length
+    # is not a whole number of 16-byte chunks, and with 9-bit digits (the
+    # 25- and 27-bit cell keys of the requested grids).
+    import torch
+    rng = np.random.default_rng(30 + offset)
+    n = 3 * 4096 + 1001
+    p = rng.uniform(0, 1000, size=(n, 3)).astype(np.float32)
+    h = rng.uniform(0, 1000, size=(1500, 3)).astype(np.float32)
+    r2 = nat.radius_table(0.001, 8, 40)
+    want = oracle.count(p, h, r2)
+    flat = torch.zeros(3 * n + 4, dtype=torch.float32, device="cuda")
+    flat[offset:offset + 3 * n] = torch.from_numpy(p.reshape(-1)).cuda()
+    dp = flat[offset:offset + 3 * n].view(n, 3)
+    torch.cuda.synchronize()
+    for grid in (None, (64, 64, 64), (256, 256, 512), (512, 512, 512)):
+        q = ctx.query(h, r2)
+        idx = ctx.build_index(dp, radius_hint=8, grid=grid)
+        q.count(idx)
+        got = q.read_counts()
+        idx.destroy()
+        q.destroy()
+        assert np.array_equal(got, want), grid
+
+
 def test_halo_struct_stride_reads_reference_layout(case_dirs, ctx):
     d, spec = case_dirs["uniform_small"]
     halos, parts = cases.load_halos_and_particles(spec, d)
