@@ -6,13 +6,16 @@ files x 1e8 uniform particles (the reference generator's MT19937 stream,
 seed 1), 1e7 uniform halos (seed 2, values as read back from the generated
 text), --radius 0.001:5:40, periodic.  A step prepares the halos (upload,
 Morton sort), then for every file builds the grid index and counts all
-halos' shells into the per-halo accumulators.  Builds of file k+1 run on the
-build stream while file k is counted on the count stream.
+halos' shells into the per-halo accumulators.  File k+1's build is queued on
+the build stream behind file k's count (its upload overlaps that count).
 
   value   halo-file passes per second (nhalos * nfiles / step time), inputs
           already resident in HBM; device time from CUDA events.
   e2e     the same through the C ABI with HOST buffers: pinned particle and
           halo buffers copied in, uint64 counts copied back every step.
+          Steps are independent jobs run as a pipeline: job k's count
+          read-back (device to host) overlaps job k+1's uploads (host to
+          device); every job's copies are inside the timed region.
   roofline  the shell-count kernel: algorithmic bytes per halo-file
           (12 + 8*nrads + 12*density*(2R)^3 = 1532 B) x halos per launch
           over its average launch time (CUDA events on the count stream).
@@ -279,10 +282,11 @@ def run_ours(args, w, dist, rank, world, local):
     ctx = nat.Context(local)
     ctx.set_overlap(args.overlap)
     # grow the device pool once, so no step takes new memory from the driver:
-    # K+1 queries, 4 indexes and one build's scratch
+    # 3 queries, a read-back's widened counts, 4 indexes, the uploaded files
+    # and one build's scratch
     idx_bytes = n * 16 + int(1.6 * n + 4096) * 4
     if not args.no_reserve:
-        ctx.reserve((args.steps + 1) * nh * (16 + 4 * nr + 48) + 4 * idx_bytes + n * 44 + (1 << 30))
+        ctx.reserve(3 * nh * (16 + 4 * nr + 48) + nh * nr * 8 + 4 * idx_bytes + nf * n * 12 + n * 44 + (1 << 30))
     s_build = torch.cuda.ExternalStream(ctx.stream(0))
     s_count = torch.cuda.ExternalStream(ctx.stream(1))
 
@@ -299,16 +303,53 @@ def run_ours(args, w, dist, rank, world, local):
             idx.destroy()
         return q
 
-    def step_e2e():
+    out_h2 = torch.empty((nh * nr,), dtype=torch.int64, pin_memory=True)
+    outs = [out_np, out_h2.numpy().view(np.uint64).reshape(nh, nr)]
+
+    def job_e2e(k):
         q = ctx.query(halos_np, r2)
         for f in range(nf):
             idx = ctx.build_index(pnp[f * n:(f + 1) * n], radius_hint=R)
             q.count(idx)
             idx.destroy()
-        q.read_counts(out=out_np, accumulate=False)
+        q.read_counts_async(outs[k & 1])
         return q
 
-    def timed(step, K, W, keep_queries):
+    def run_e2e(jobs):
+        # at most two jobs in flight: job k is queued before job k-1's
+        # read-back is awaited, so the two overlap on the copy engines
+        prev = None
+        for k in range(jobs):
+            q = job_e2e(k)
+            if prev is not None:
+                prev.wait_read()
+                prev.destroy()
+            prev = q
+        if prev is not None:
+            prev.wait_read()
+            prev.destroy()
+
+    def timed_e2e(K, W):
+        run_e2e(W)
+        dist_barrier(dist, local)
+        torch.cuda.synchronize()
+        ctx.sync()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        l0 = nat.launch_counter()
+        with ClockSampler(local) as clk:
+            e0.record(s_count)
+            s_build.wait_event(e0)
+            run_e2e(K)
+            # recorded after the last read-back was seen complete on the host
+            e1.record(s_count)
+            e1.synchronize()
+        launches = nat.launch_counter() - l0
+        ctx.sync()
+        torch.cuda.synchronize()
+        dist_barrier(dist, local)
+        return e0.elapsed_time(e1) / K, launches, clk.summary()
+
+    def timed(step, K, W):
         for _ in range(W):
             q = step()
             ctx.sync()
@@ -321,16 +362,16 @@ def run_ours(args, w, dist, rank, world, local):
         with ClockSampler(local) as clk:
             e0.record(s_count)
             s_build.wait_event(e0)
-            qs = []
+            cnt_ms, calls = 0.0, 0
             for _ in range(K):
                 q = step()
                 # a step is one job: the next one starts when this one is done,
                 # so builds never run ahead into the next step's files
                 q.wait()
-                if keep_queries:
-                    qs.append(q)
-                else:
-                    q.destroy()
+                t = q.timing()  # event pairs already complete: no wait
+                cnt_ms += t["count_ms"]
+                calls += t["count_calls"]
+                q.destroy()
             e1.record(s_count)
             e1.synchronize()
         launches = nat.launch_counter() - l0
@@ -338,21 +379,15 @@ def run_ours(args, w, dist, rank, world, local):
         torch.cuda.synchronize()
         dist_barrier(dist, local)
         ms = e0.elapsed_time(e1) / K
-        cnt_ms, calls = 0.0, 0
-        for q in qs:
-            t = q.timing()
-            cnt_ms += t["count_ms"]
-            calls += t["count_calls"]
-            q.destroy()
         return ms, launches, (cnt_ms / calls if calls else None), clk.summary()
 
     K, W = args.steps, args.warmup
-    ms, launches, count_ms, clocks = timed(step_resident, K, W, keep_queries=True)
+    ms, launches, count_ms, clocks = timed(step_resident, K, W)
     ms = dist_max(dist, ms, local)
     if args.no_e2e:
         ms_e2e, launches_e2e, clocks_e2e = float("nan"), 0, None
     else:
-        ms_e2e, launches_e2e, _, clocks_e2e = timed(step_e2e, K, W, keep_queries=False)
+        ms_e2e, launches_e2e, clocks_e2e = timed_e2e(K, W)
         ms_e2e = dist_max(dist, ms_e2e, local)
 
     # one extra untimed pass for the per-phase split (build vs search)
@@ -437,7 +472,8 @@ def run_ours(args, w, dist, rank, world, local):
         "e2e": None if args.no_e2e else {
             "value": round(e2e_value, 1), "unit": UNIT, "ms_per_step": round(ms_e2e, 3),
             "h2d_bytes_per_step": int(nf * n * 12 + (nh - 1) * 24 + 12),
-            "d2h_bytes_per_step": int(nh * nr * 8)},
+            "d2h_bytes_per_step": int(nh * nr * 8),
+            "pipeline": "job k's read-back overlaps job k+1's uploads (2 jobs in flight)"},
         "roofline": roof,
         "cpu_baseline": cpu,
         "clocks": clocks,

@@ -264,6 +264,21 @@ int sjcs_query_wait(sjcs_query *q);
  * reference's += on its calloc'd ulong_t array, src/astr_rcount/main.c:651),
  * accumulate == 0 overwrites.  Blocks until the copy is done. */
 int sjcs_query_read_counts(sjcs_ctx *ctx, sjcs_query *q, uint64_t *counts, int accumulate);
+/* Queue a read-back of the accumulated counts (uint64 [nhalos][nrads], caller's
+ * halo order, overwriting) into page-locked host memory (cudaMallocHost,
+ * cudaHostRegister or sjcs_host_alloc) and return at once.  The copy runs on
+ * the context's read-back stream after every count queued on q so far, so it
+ * overlaps uploads and builds queued afterwards (host-to-device and
+ * device-to-host copies use separate copy engines).  The counts are in place
+ * when sjcs_query_wait_read returns; until then `counts` must stay valid.
+ * Later counts, resets and sjcs_query_destroy on q wait for the read on the
+ * device.  Non-page-locked `counts` fail with SJCS_ERR_INVALID.  The
+ * asynchronous form of sjcs_query_read_counts(..., accumulate = 0); the
+ * reference reads its counts in place after the last file (main.c:651). */
+int sjcs_query_read_counts_async(sjcs_ctx *ctx, sjcs_query *q, uint64_t *counts);
+/* Block until the last read queued by sjcs_query_read_counts_async on q is in
+ * host memory (returns at once when none is pending). */
+int sjcs_query_wait_read(sjcs_query *q);
 /* Device pointer to the query's uint32 accumulators [nhalos][nrads] in the
  * order the halos were given (valid until sjcs_query_destroy). */
 int sjcs_query_device_counts(const sjcs_query *q, uint32_t **d_counts);

@@ -128,6 +128,8 @@ _SIGS = {
     "sjcs_query_count": (_c.c_int, [_vp, _vp, _vp]),
     "sjcs_query_wait": (_c.c_int, [_vp]),
     "sjcs_query_read_counts": (_c.c_int, [_vp, _vp, _vp, _c.c_int]),
+    "sjcs_query_read_counts_async": (_c.c_int, [_vp, _vp, _vp]),
+    "sjcs_query_wait_read": (_c.c_int, [_vp]),
     "sjcs_query_device_counts": (_c.c_int, [_vp, _pp]),
     "sjcs_query_reset": (_c.c_int, [_vp, _vp]),
     "sjcs_query_timing": (_c.c_int, [_vp, _c.POINTER(sjcs_timing)]),
@@ -497,6 +499,7 @@ class Query:
         self.nhalos = nhalos
         self.nrads = nrads
         self._keep = keep
+        self._reading = None
 
     def count(self, index: Index) -> "Query":
         _check(lib().sjcs_query_count(self.ctx._h, self._h, index._h))
@@ -513,6 +516,20 @@ class Query:
             raise ValueError("out must be a C-contiguous uint64 array of nhalos*nrads elements")
         _check(lib().sjcs_query_read_counts(self.ctx._h, self._h, _vp(_ptr(out)), 1 if accumulate else 0))
         return out
+
+    def read_counts_async(self, out: np.ndarray) -> np.ndarray:
+        """Queue a read of the counts into page-locked `out` (a PinnedBuffer's
+        uint64 array of nhalos*nrads elements) and return at once; the counts
+        are there after wait_read()."""
+        if out.dtype != np.uint64 or not out.flags.c_contiguous or out.size != self.nhalos * self.nrads:
+            raise ValueError("out must be a C-contiguous uint64 array of nhalos*nrads elements")
+        _check(lib().sjcs_query_read_counts_async(self.ctx._h, self._h, _vp(_ptr(out))))
+        self._reading = out  # keep the destination alive while the copy runs
+        return out
+
+    def wait_read(self) -> None:
+        _check(lib().sjcs_query_wait_read(self._h))
+        self._reading = None
 
     def read_counts_into(self, ptr: int, accumulate: bool = False) -> None:
         """Read into caller memory given by address (e.g. a pinned torch tensor)."""

@@ -194,12 +194,20 @@ sjcs_query* new_query(sjcs_ctx* ctx) {
     cudaEventCreate(&q->ev_last);
     cudaEventCreate(&q->ev_d0);
     cudaEventCreate(&q->ev_d1);
+    cudaEventCreateWithFlags(&q->ev_rq, cudaEventDisableTiming);
     return q;
+}
+
+// Work that writes or frees q's counts waits, on stream s, for an
+// asynchronous read of them (a no-op once the read has finished).
+cudaError_t after_reads(const sjcs_query* q, cudaStream_t s) {
+    return q->read_queued ? cudaStreamWaitEvent(s, q->ev_d1, 0) : cudaSuccess;
 }
 
 void free_query(sjcs_query* q) {
     if (!q) return;
     cudaStream_t s = q->ctx->s_count;
+    after_reads(q, s);
     if (q->halos) cudaFreeAsync(q->halos, s);
     if (q->counts) cudaFreeAsync(q->counts, s);
     if (q->d_r2) cudaFreeAsync(q->d_r2, s);
@@ -210,6 +218,7 @@ void free_query(sjcs_query* q) {
     cudaEventDestroy(q->ev_last);
     cudaEventDestroy(q->ev_d0);
     cudaEventDestroy(q->ev_d1);
+    cudaEventDestroy(q->ev_rq);
     q->magic = 0;
     delete q;
 }
@@ -285,6 +294,33 @@ int enqueue_build(sjcs_ctx* ctx, sjcs_index* idx, const float* d_xyz, uint64_t n
     return build_grid_index(ctx, d_xyz, n, auto_grid(n, o.radius_hint, o.grid), idx, s);
 }
 
+// Copy a host file to new device memory on the upload stream and make the
+// build stream wait for it: uploads of later files never queue behind builds
+// that wait for counts, so the copy engine stays busy.  idx's ev_start and
+// ev_h2d bracket the copy.  The caller frees *d on the build stream.
+int upload(sjcs_ctx* ctx, sjcs_index* idx, const void* host, size_t bytes, void** d) {
+    cudaStream_t u = ctx->s_h2d;
+    *d = nullptr;
+    cudaEventRecord(idx->ev_start, u);
+    cudaError_t e = cudaMallocAsync(d, bytes, u);
+    if (e != cudaSuccess) {
+        *d = nullptr;
+        cudaGetLastError();
+        return fail(SJCS_ERR_NOMEM, "device allocation of %llu bytes for the upload failed: %s",
+                    (unsigned long long)bytes, cudaGetErrorString(e));
+    }
+    e = cudaMemcpyAsync(*d, host, bytes, cudaMemcpyHostToDevice, u);
+    if (e == cudaSuccess) e = cudaEventRecord(idx->ev_h2d, u);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->s_build, idx->ev_h2d, 0);
+    if (e != cudaSuccess) {
+        cudaFreeAsync(*d, u);
+        *d = nullptr;
+        return fail(SJCS_ERR_CUDA, "host-to-device copy failed: %s", cudaGetErrorString(e));
+    }
+    idx->had_h2d = true;
+    return SJCS_OK;
+}
+
 int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, const sjcs_index_opts* opts,
                        sjcs_index** out) {
     if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
@@ -303,28 +339,22 @@ int index_build_common(sjcs_ctx* ctx, const float* xyz, bool host, uint64_t n, c
     idx->kind = o.kind;
     idx->n = n;
     cudaStream_t s = ctx->s_build;
-    cudaEventRecord(idx->ev_start, s);
     const float* d_xyz = xyz;
-    StreamScratch scr(s);
+    void* up = nullptr;
     if (host && n) {
-        float* d = nullptr;
-        cudaError_t e = scr.alloc(&d, n * 3 * sizeof(float));
-        if (e != cudaSuccess) {
+        rc = upload(ctx, idx, xyz, n * 3 * sizeof(float), &up);
+        if (rc) {
             free_index(idx);
-            return fail(SJCS_ERR_NOMEM, "device allocation of %llu particles failed: %s", (unsigned long long)n,
-                        cudaGetErrorString(e));
+            return rc;
         }
-        e = cudaMemcpyAsync(d, xyz, n * 3 * sizeof(float), cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) {
-            free_index(idx);
-            return fail(SJCS_ERR_CUDA, "host-to-device copy failed: %s", cudaGetErrorString(e));
-        }
-        d_xyz = d;
-        idx->had_h2d = true;
+        d_xyz = static_cast<const float*>(up);
+    } else {
+        cudaEventRecord(idx->ev_start, s);
+        cudaEventRecord(idx->ev_h2d, s);
     }
-    cudaEventRecord(idx->ev_h2d, s);
     order_after_counts(ctx, s);
     rc = enqueue_build(ctx, idx, d_xyz, n, o, s);
+    if (up) cudaFreeAsync(up, s);  // after the build, in stream order
     if (rc) {
         free_index(idx);
         return rc;
@@ -452,6 +482,8 @@ int sjcs_ctx_create(int device, sjcs_ctx** out) {
     cudaDeviceGetAttribute(&ctx->num_sms, cudaDevAttrMultiProcessorCount, device);
     SJCS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->s_build, cudaStreamNonBlocking));
     SJCS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->s_count, cudaStreamNonBlocking));
+    SJCS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->s_read, cudaStreamNonBlocking));
+    SJCS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->s_h2d, cudaStreamNonBlocking));
     SJCS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_counts, cudaEventDisableTiming));
     // Keep freed stream-ordered memory cached in the pool: every file's index
     // and scratch reuse the previous file's pages without new cudaMalloc calls.
@@ -470,8 +502,12 @@ int sjcs_ctx_destroy(sjcs_ctx* ctx) {
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->s_build);
     cudaStreamSynchronize(ctx->s_count);
+    cudaStreamSynchronize(ctx->s_read);
+    cudaStreamSynchronize(ctx->s_h2d);
     cudaStreamDestroy(ctx->s_build);
     cudaStreamDestroy(ctx->s_count);
+    cudaStreamDestroy(ctx->s_read);
+    cudaStreamDestroy(ctx->s_h2d);
     if (ctx->ev_counts) cudaEventDestroy(ctx->ev_counts);
     ctx->magic = 0;
     delete ctx;
@@ -484,6 +520,8 @@ int sjcs_ctx_sync(sjcs_ctx* ctx) {
     if (rc) return rc;
     SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_build));
     SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_count));
+    SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_read));
+    SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_h2d));
     return SJCS_OK;
 }
 
@@ -606,29 +644,31 @@ int sjcs_index_build_compressed(sjcs_ctx* ctx, const uint16_t* uv, uint64_t n, c
     idx->kind = o.kind;
     idx->n = n;
     cudaStream_t s = ctx->s_build;
-    cudaEventRecord(idx->ev_start, s);
+    void* up = nullptr;
+    if (n) {
+        rc = upload(ctx, idx, uv, n * 3 * sizeof(uint16_t), &up);
+        if (rc) {
+            free_index(idx);
+            return rc;
+        }
+    } else {
+        cudaEventRecord(idx->ev_start, s);
+        cudaEventRecord(idx->ev_h2d, s);
+    }
+    const uint16_t* d_uv = static_cast<const uint16_t*>(up);
     StreamScratch scr(s);
-    uint16_t* d_uv = nullptr;
     float* d_xyz = nullptr;
-    cudaError_t e = scr.alloc(&d_uv, n * 3 * sizeof(uint16_t));
-    if (e == cudaSuccess) e = scr.alloc(&d_xyz, n * 3 * sizeof(float));
+    cudaError_t e = scr.alloc(&d_xyz, n * 3 * sizeof(float));
     if (e != cudaSuccess) {
+        if (up) cudaFreeAsync(up, s);
         free_index(idx);
         return fail(SJCS_ERR_NOMEM, "device allocation for %llu compressed particles failed: %s",
                     (unsigned long long)n, cudaGetErrorString(e));
     }
-    if (n) {
-        e = cudaMemcpyAsync(d_uv, uv, n * 3 * sizeof(uint16_t), cudaMemcpyHostToDevice, s);
-        if (e != cudaSuccess) {
-            free_index(idx);
-            return fail(SJCS_ERR_CUDA, "host-to-device copy failed: %s", cudaGetErrorString(e));
-        }
-        idx->had_h2d = true;
-    }
-    cudaEventRecord(idx->ev_h2d, s);
     order_after_counts(ctx, s);
     rc = launch_decode(d_uv, n, g, d_xyz, s);
     if (!rc) rc = enqueue_build(ctx, idx, d_xyz, n, o, s);
+    if (up) cudaFreeAsync(up, s);  // after the decode, in stream order
     if (rc) {
         free_index(idx);
         return rc;
@@ -787,6 +827,7 @@ int sjcs_query_count(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx) {
     std::lock_guard<std::mutex> lk(ctx->mu);
     cudaStream_t s = ctx->s_count;
     SJCS_CUDA_TRY(cudaStreamWaitEvent(s, idx->ev_ready, 0));
+    SJCS_CUDA_TRY(after_reads(q, s));
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     SJCS_CUDA_TRY(cudaEventCreate(&e0));
     SJCS_CUDA_TRY(cudaEventCreate(&e1));
@@ -891,6 +932,7 @@ int sjcs_step_launch(sjcs_ctx* ctx, sjcs_step* st) {
     // earlier counts and read-backs of the query)
     SJCS_CUDA_TRY(cudaEventRecord(st->ev_pre, ctx->s_count));
     SJCS_CUDA_TRY(cudaStreamWaitEvent(ctx->s_build, st->ev_pre, 0));
+    SJCS_CUDA_TRY(after_reads(st->q, ctx->s_build));
     SJCS_CUDA_TRY(cudaEventRecord(st->ev0, ctx->s_build));
     SJCS_CUDA_TRY(cudaGraphLaunch(st->exec, ctx->s_build));
     for (size_t k = 0; k < st->kernels; ++k) note_launch();
@@ -1082,6 +1124,43 @@ int sjcs_query_read_counts(sjcs_ctx* ctx, sjcs_query* q, uint64_t* counts, int a
     return SJCS_OK;
 }
 
+int sjcs_query_read_counts_async(sjcs_ctx* ctx, sjcs_query* q, uint64_t* counts) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_query(q) || q->ctx != ctx) return fail(SJCS_ERR_STATE, "query does not belong to this context");
+    const uint64_t m = q->nhalos * (uint64_t)q->nrads;
+    if (m == 0) return SJCS_OK;
+    if (!counts) return fail(SJCS_ERR_INVALID, "counts is NULL");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    if (!is_pinned(counts) || !is_pinned(counts + (m - 1)))
+        return fail(SJCS_ERR_INVALID, "counts must be page-locked host memory for an asynchronous read");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t s = ctx->s_read;
+    // after everything queued on the count stream so far: q's upload and counts
+    SJCS_CUDA_TRY(cudaEventRecord(q->ev_rq, ctx->s_count));
+    SJCS_CUDA_TRY(cudaStreamWaitEvent(s, q->ev_rq, 0));
+    StreamScratch scr(s);  // freed in stream order after the copy
+    unsigned long long* wide = nullptr;
+    SJCS_CUDA_TRY(scr.alloc(&wide, m * sizeof(uint64_t)));
+    SJCS_CUDA_TRY(cudaEventRecord(q->ev_d0, s));
+    k_widen_u32_u64<<<ctx->num_sms * 8, 256, 0, s>>>(q->counts, m, wide);
+    SJCS_LAUNCH_CHECK();
+    SJCS_CUDA_TRY(cudaMemcpyAsync(counts, wide, m * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    SJCS_CUDA_TRY(cudaEventRecord(q->ev_d1, s));
+    q->read_queued = true;
+    return SJCS_OK;
+}
+
+int sjcs_query_wait_read(sjcs_query* q) {
+    if (!valid_query(q)) return fail(SJCS_ERR_STATE, "invalid query");
+    if (!q->read_queued) return SJCS_OK;
+    SJCS_CUDA_TRY(cudaEventSynchronize(q->ev_d1));
+    float ms = 0.f;
+    q->last_d2h_ms = (cudaEventElapsedTime(&ms, q->ev_d0, q->ev_d1) == cudaSuccess) ? ms : 0.f;
+    cudaGetLastError();
+    return SJCS_OK;
+}
+
 int sjcs_query_device_counts(const sjcs_query* q, uint32_t** d_counts) {
     if (!valid_query(q) || !d_counts) return fail(SJCS_ERR_INVALID, "invalid argument");
     *d_counts = q->counts;
@@ -1095,6 +1174,7 @@ int sjcs_query_reset(sjcs_ctx* ctx, sjcs_query* q) {
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(ctx->mu);
     const uint64_t m = q->nhalos * (uint64_t)q->nrads;
+    SJCS_CUDA_TRY(after_reads(q, ctx->s_count));
     if (m) SJCS_CUDA_TRY(cudaMemsetAsync(q->counts, 0, m * sizeof(uint32_t), ctx->s_count));
     SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_count));
     clear_count_events(q);

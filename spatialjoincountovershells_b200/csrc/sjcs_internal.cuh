@@ -119,6 +119,8 @@ struct sjcs_ctx {
     int num_sms;
     cudaStream_t s_build;  // particle copies + index builds
     cudaStream_t s_count;  // halo upload/sort, shell counts, count read-back
+    cudaStream_t s_read = nullptr;  // asynchronous count read-back
+    cudaStream_t s_h2d = nullptr;   // uploads of host particle files
     std::mutex mu;
     std::map<std::string, sjcs_schedule> tuned;  // autotuned schedules by workload shape
     bool overlap = false;    // builds' kernels may run beside queued counts
@@ -173,6 +175,8 @@ struct sjcs_query {
     std::vector<cudaEvent_t> count_events;  // (start, end) pairs, one per count call since reset
     cudaEvent_t ev_last;                    // end of the last count call
     cudaEvent_t ev_d0, ev_d1;
+    cudaEvent_t ev_rq = nullptr;  // s_count's work when an asynchronous read was queued
+    bool read_queued = false;     // an asynchronous read ended at ev_d1 (maybe still running)
     float last_d2h_ms;
     sjcs_schedule sched;  // count schedule (SJCS_SCHED_AUTO by default)
 };
