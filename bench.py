@@ -496,6 +496,8 @@ CLUSTERED = dict(workload="clustered", nfiles=3, nparticles=100_000_000, nhalos=
 FORMS = dict(CLUSTERED, workload="learned", radius=(0.001, 5.0, 40))
 SERVING = dict(workload="serving", nfiles=3, nparticles=100_000_000, nrequests=2000, size=(1e2, 1e6),
                nrads=(8, 64), rmax=(1.0, 10.0), arrival_seed=51, pseed=31, hseed=32)
+IO = dict(workload="io", nfiles=1, nparticles=100_000_000, nhalos=1_000_000, radius=(0.001, 5.0, 40),
+          pseed=1, hseed=2)
 
 
 def clustered_name(w) -> str:
@@ -781,6 +783,67 @@ def run_forms(args, w, dist, rank, world, local):
     return line
 
 
+def run_io(args, w, dist, rank, world, local):
+    """The host phases around the GPU path, as the driver runs them: halo text
+    ingest (readHalos), particle file read (readDecodedParticles) and result
+    text output (outputResult), from the phase lines sjcs_rcount prints like
+    astr_rcount does, on the same files.  The reference program's own phase
+    lines on this host's cores are the cpu_baseline."""
+    import subprocess
+
+    from spatialjoincountovershells_b200 import _native as nat
+    driver = ROOT / "spatialjoincountovershells_b200" / "bin" / "sjcs_rcount"
+    if not driver.exists():
+        raise RuntimeError(f"{driver} is missing; run python -m spatialjoincountovershells_b200.build")
+    if rank != 0:
+        return None
+    T = ref_threads()
+    mn, mx, nr = w["radius"]
+    phases = ["halo data reading", "particles reading", "result writing"]
+
+    def run(cmd, cwd):
+        t0 = time.time()
+        r = subprocess.run([str(c) for c in cmd], cwd=cwd, capture_output=True, text=True, timeout=3600)
+        wall = time.time() - t0
+        if r.returncode != 0:
+            raise RuntimeError(f"{cmd[0]} failed: {r.stderr[-500:]}")
+        t = {}
+        for m in re.finditer(r">>>> (.+?) time: (\d+) milli seconds", r.stdout):
+            t[m.group(1)] = t.get(m.group(1), 0) + int(m.group(2))
+        return t, wall
+
+    with tempfile.TemporaryDirectory(prefix="sjcs_io_") as td:
+        d = pathlib.Path(td)
+        pf, hf = d / "part0.dat", d / "halos.list"
+        nat.write_particle_file(pf, nat.gen_uniform_particles(w["pseed"], 1, w["nparticles"]))
+        nat.gen_uniform_halo_file(hf, w["hseed"], w["nhalos"])
+        cli = ["--thread", T, "--next-setup", T, "--particle-files", pf.name, "--halo-file", hf.name,
+               "--radius", f"{mn}:{mx}:{nr}"]
+        ours, ours_wall = run([driver, *cli, "--output-file", "ours.txt"], d)
+        out_bytes = (d / "ours.txt").stat().st_size
+        (d / "ours.txt").unlink()
+        cpu = None
+        if not args.no_cpu_baseline:
+            from oracle import oracle
+            if oracle.ref_available():
+                ref, ref_wall = run([oracle.REF_ASTR, *cli, "--output-file", "ref.txt"], d)
+                cpu = {"value": sum(ref.get(k, 0) for k in phases), "unit": "ms", "cores": T, "kind": "reference",
+                       "sample": "the whole workload", "phases_ms": {k: ref.get(k) for k in phases},
+                       "wall_s": round(ref_wall, 2)}
+    total = sum(ours.get(k, 0) for k in phases)
+    return {
+        "metric": "host phases of one driver run: halo text read + particle file read + result text write",
+        "value": total, "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 0, "ms_per_step": total,
+        "higher_is_better": False, "scaling": "weak", "vs_baseline": None, "dtype": "f32 / text",
+        "data": "synthetic: reference generator streams",
+        "config": {"workload": f"io: {w['nfiles']} file x {w['nparticles']:.0e} uniform particles "
+                               f"(seed {w['pseed']}), {w['nhalos']:.0e} halos (seed {w['hseed']}), "
+                               f"--radius {mn}:{mx}:{nr}, --thread {T}", "parallelism": "host threads"},
+        "phases_ms": {k: ours.get(k) for k in phases}, "all_phases_ms": ours, "wall_s": round(ours_wall, 2),
+        "result_text_bytes": out_bytes, "cpu_baseline": cpu,
+    }
+
+
 def run_serving(args, w, dist, rank, world, local):
     """C5: request loop over resident clustered indexes, Poisson arrivals, p50/p99."""
     import numpy as np
@@ -985,9 +1048,10 @@ def main():
     ap.add_argument("--particles", type=int, default=None, help="override particles per file (profiling cases)")
     ap.add_argument("--no-reserve", action="store_true",
                     help="do not grow the device memory pool up front (profiling cases: keep the footprint small)")
-    ap.add_argument("--workload", choices=["uniform", "clustered", "learned", "serving"], default="uniform",
+    ap.add_argument("--workload", choices=["uniform", "clustered", "learned", "serving", "io"], default="uniform",
                     help="uniform: the headline line (README scale); clustered: persistent schedule and captured "
-                         "steps; learned: index forms on clustered data; serving: the request loop")
+                         "steps; learned: index forms on clustered data; serving: the request loop; "
+                         "io: the driver's host phases (halo text read, particle read, result write)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -1006,7 +1070,7 @@ def main():
         return
     dist, rank, world, local = dist_setup()
     if args.workload != "uniform":
-        base = {"clustered": CLUSTERED, "learned": FORMS, "serving": SERVING}[args.workload]
+        base = {"clustered": CLUSTERED, "learned": FORMS, "serving": SERVING, "io": IO}[args.workload]
         w = dict(base)
         if args.small:
             w["nparticles"] //= 50
@@ -1021,10 +1085,11 @@ def main():
             w["nhalos"] = args.halos
         if args.particles:
             w["nparticles"] = args.particles
-        run = {"clustered": run_clustered, "learned": run_forms, "serving": run_serving}[args.workload]
+        run = {"clustered": run_clustered, "learned": run_forms, "serving": run_serving,
+               "io": run_io}[args.workload]
         line = run(args, w, dist, rank, world, local)
         dist_close(dist)
-        if rank == 0:
+        if rank == 0 and line is not None:
             print(json.dumps(line), flush=True)
         return
     line = run_ours(args, w, dist, rank, world, local)

@@ -201,6 +201,15 @@ int sjcs_index_build(sjcs_ctx *ctx, const float *xyz, uint64_t n,
 /* Same, with the particles already in device memory (d_xyz, n*3 floats). */
 int sjcs_index_build_device(sjcs_ctx *ctx, const float *d_xyz, uint64_t n,
                             const sjcs_index_opts *opts, sjcs_index **out);
+/* Same, reading a decoded particle file (x,y,z float triplets, count =
+ * file size / 12, as readDecodedParticles, src/Gadget/BufVector3D.c:285-308).
+ * Several threads read the file in 16 MB chunks into a small page-locked
+ * staging area owned by the context (allocated on first use) and each chunk is
+ * copied to the device as soon as it is read, so no page-locked copy of the
+ * whole file is made and reading overlaps the upload.  Returns once the file
+ * is read and the copies and the build are queued.  A missing or unreadable
+ * file fails with SJCS_ERR_INVALID. */
+int sjcs_index_build_file(sjcs_ctx *ctx, const char *path, const sjcs_index_opts *opts, sjcs_index **out);
 /* Same, from compressed (Gadget-encoded) particles: n uint16 triplets in HOST
  * memory (the displacement record of a compressed file) and the file's
  * 256-byte header (the layout of GadgetHeader, include/Gadget/GadgetHeader.h:4-27;

@@ -127,6 +127,7 @@ _SIGS = {
     "sjcs_query_create_device": (_c.c_int, [_vp, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _pp]),
     "sjcs_query_count": (_c.c_int, [_vp, _vp, _vp]),
     "sjcs_query_wait": (_c.c_int, [_vp]),
+    "sjcs_index_build_file": (_c.c_int, [_vp, _c.c_char_p, _c.POINTER(sjcs_index_opts), _pp]),
     "sjcs_query_read_counts": (_c.c_int, [_vp, _vp, _vp, _c.c_int]),
     "sjcs_query_read_counts_async": (_c.c_int, [_vp, _vp, _vp]),
     "sjcs_query_wait_read": (_c.c_int, [_vp]),
@@ -303,6 +304,15 @@ class Context:
                                           _c.byref(h)))
             keep = arr
         return Index(self, h, keep)
+
+    def build_index_file(self, path, radius_hint: float = 0.0, grid=None, kind: int = INDEX_GRID, level: int = 0,
+                         verify: bool = False) -> "Index":
+        """Index over a decoded particle file, read in chunks that are uploaded
+        as they are read (no page-locked copy of the whole file)."""
+        opts = _make_opts(radius_hint, grid, kind, level, verify)
+        h = _vp()
+        _check(lib().sjcs_index_build_file(self._h, os.fsencode(str(path)), _c.byref(opts), _c.byref(h)))
+        return Index(self, h, None)
 
     def build_index_compressed(self, uv, header: bytes, radius_hint: float = 0.0, kind: int = INDEX_GRID,
                                level: int = 0) -> "Index":

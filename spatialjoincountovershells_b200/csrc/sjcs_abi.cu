@@ -1,4 +1,8 @@
 // extern "C" entry points of libsjcs.so (declared in include/sjcs.h).
+#include <fcntl.h>
+#include <sys/stat.h>
+#include <unistd.h>
+
 #include <algorithm>
 #include <atomic>
 #include <cmath>
@@ -508,6 +512,9 @@ int sjcs_ctx_destroy(sjcs_ctx* ctx) {
     cudaStreamDestroy(ctx->s_count);
     cudaStreamDestroy(ctx->s_read);
     cudaStreamDestroy(ctx->s_h2d);
+    for (cudaEvent_t e : ctx->ring_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->ring) cudaFreeHost(ctx->ring);
     if (ctx->ev_counts) cudaEventDestroy(ctx->ev_counts);
     ctx->magic = 0;
     delete ctx;
@@ -621,6 +628,138 @@ int sjcs_index_build(sjcs_ctx* ctx, const float* xyz, uint64_t n, const sjcs_ind
 int sjcs_index_build_device(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const sjcs_index_opts* opts,
                             sjcs_index** out) {
     return index_build_common(ctx, d_xyz, false, n, opts, out);
+}
+
+namespace {
+constexpr size_t kIngestChunk = 16u << 20;  // bytes per read and per copy
+constexpr unsigned kIngestThreads = 8;      // reader threads = staging slots
+
+// Read [off, off + len) of fd completely.
+bool pread_all(int fd, char* dst, uint64_t off, uint64_t len) {
+    uint64_t done = 0;
+    while (done < len) {
+        const ssize_t r = pread(fd, dst + done, (size_t)(len - done), (off_t)(off + done));
+        if (r <= 0) return false;
+        done += (uint64_t)r;
+    }
+    return true;
+}
+
+// bytes of fd into new device memory *d on the upload stream: reader thread t
+// takes chunks t, t + T, ... through its own staging slot, waiting for the
+// slot's previous copy before overwriting it.  idx's ev_start / ev_h2d
+// bracket the copies and the build stream waits for them.  Called with
+// ctx->ring_mu held.
+int ingest_file(sjcs_ctx* ctx, sjcs_index* idx, int fd, uint64_t bytes, void** d) {
+    cudaStream_t u = ctx->s_h2d;
+    const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
+    const unsigned T = std::min(kIngestThreads, hw);
+    if (!ctx->ring) {
+        SJCS_CUDA_TRY(cudaMallocHost(&ctx->ring, (size_t)kIngestThreads * kIngestChunk));
+        ctx->ring_ev.assign(kIngestThreads, nullptr);
+        for (auto& e : ctx->ring_ev) SJCS_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    *d = nullptr;
+    cudaEventRecord(idx->ev_start, u);
+    cudaError_t e = cudaMallocAsync(d, bytes, u);
+    if (e != cudaSuccess) {
+        *d = nullptr;
+        cudaGetLastError();
+        return fail(SJCS_ERR_NOMEM, "device allocation of %llu bytes for the file failed: %s",
+                    (unsigned long long)bytes, cudaGetErrorString(e));
+    }
+    const uint64_t nchunks = (bytes + kIngestChunk - 1) / kIngestChunk;
+    std::atomic<int> bad_read{0}, bad_cuda{0};
+    auto worker = [&](unsigned t) {
+        char* slot = ctx->ring + (size_t)t * kIngestChunk;
+        for (uint64_t c = t; c < nchunks && !bad_read && !bad_cuda; c += T) {
+            const uint64_t off = c * kIngestChunk, len = std::min<uint64_t>(kIngestChunk, bytes - off);
+            if (cudaEventSynchronize(ctx->ring_ev[t]) != cudaSuccess) { bad_cuda = 1; return; }
+            if (!pread_all(fd, slot, off, len)) { bad_read = 1; return; }
+            if (cudaMemcpyAsync(static_cast<char*>(*d) + off, slot, len, cudaMemcpyHostToDevice, u) != cudaSuccess ||
+                cudaEventRecord(ctx->ring_ev[t], u) != cudaSuccess) {
+                bad_cuda = 1;
+                return;
+            }
+        }
+    };
+    std::vector<std::thread> th;
+    th.reserve(T);
+    for (unsigned t = 1; t < T; ++t) th.emplace_back(worker, t);
+    worker(0);
+    for (auto& x : th) x.join();
+    if (bad_read || bad_cuda) {
+        cudaStreamSynchronize(u);  // copies out of the staging slots are done before they are reused
+        cudaFreeAsync(*d, u);
+        *d = nullptr;
+        cudaGetLastError();
+        return bad_read ? fail(SJCS_ERR_INVALID, "short read of the particle file")
+                        : fail(SJCS_ERR_CUDA, "host-to-device copy of the particle file failed");
+    }
+    cudaEventRecord(idx->ev_h2d, u);
+    SJCS_CUDA_TRY(cudaStreamWaitEvent(ctx->s_build, idx->ev_h2d, 0));
+    idx->had_h2d = true;
+    return SJCS_OK;
+}
+}  // namespace
+
+int sjcs_index_build_file(sjcs_ctx* ctx, const char* path, const sjcs_index_opts* opts, sjcs_index** out) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!out) return fail(SJCS_ERR_INVALID, "out is NULL");
+    *out = nullptr;
+    if (!path) return fail(SJCS_ERR_INVALID, "path is NULL");
+    sjcs_index_opts o{};
+    int rc = check_opts(opts, &o);
+    if (rc) return rc;
+    const int fd = open(path, O_RDONLY);
+    struct stat st;
+    if (fd < 0 || fstat(fd, &st) != 0) {
+        if (fd >= 0) close(fd);
+        return fail(SJCS_ERR_INVALID, "ERROR: file %s not found in readDecodedParticles()", path);
+    }
+    const uint64_t n = (uint64_t)st.st_size / (3 * sizeof(float));
+    if (n > 0xffffffffull) {
+        close(fd);
+        return fail(SJCS_ERR_INVALID, "too many particles for one index (%llu)", (unsigned long long)n);
+    }
+    rc = set_device(ctx);
+    if (rc) {
+        close(fd);
+        return rc;
+    }
+    sjcs_index* idx = new_index(ctx);
+    if (!idx) {
+        close(fd);
+        return fail(SJCS_ERR_NOMEM, "out of host memory");
+    }
+    idx->kind = o.kind;
+    idx->n = n;
+    void* d = nullptr;
+    if (n) {
+        std::lock_guard<std::mutex> lk(ctx->ring_mu);
+        rc = ingest_file(ctx, idx, fd, n * 3 * sizeof(float), &d);
+    }
+    close(fd);
+    if (rc) {
+        free_index(idx);
+        return rc;
+    }
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    cudaStream_t s = ctx->s_build;
+    if (!n) {
+        cudaEventRecord(idx->ev_start, s);
+        cudaEventRecord(idx->ev_h2d, s);
+    }
+    order_after_counts(ctx, s);
+    rc = enqueue_build(ctx, idx, static_cast<const float*>(d), n, o, s);
+    if (d) cudaFreeAsync(d, s);  // after the build, in stream order
+    if (rc) {
+        free_index(idx);
+        return rc;
+    }
+    cudaEventRecord(idx->ev_ready, s);
+    *out = idx;
+    return SJCS_OK;
 }
 
 int sjcs_index_build_compressed(sjcs_ctx* ctx, const uint16_t* uv, uint64_t n, const void* gadget_header,

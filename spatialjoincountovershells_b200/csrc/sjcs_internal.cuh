@@ -125,6 +125,11 @@ struct sjcs_ctx {
     std::map<std::string, sjcs_schedule> tuned;  // autotuned schedules by workload shape
     bool overlap = false;    // builds' kernels may run beside queued counts
     cudaEvent_t ev_counts = nullptr;  // marks the counts queued so far (build ordering)
+    // File ingest (sjcs_index_build_file): pinned staging slots, one per
+    // reader thread, each with the event of the last copy out of it.
+    std::mutex ring_mu;
+    char* ring = nullptr;
+    std::vector<cudaEvent_t> ring_ev;
 };
 
 namespace sjcs {

@@ -62,10 +62,38 @@ int sjcs_particle_file_count(const char *path, uint64_t *n)
     return 0;
 }
 
+typedef struct ReadJob {
+    int fd;
+    char *dst;
+    uint64_t off, len;
+    int bad;
+} ReadJob;
+
+static void *read_job(void *arg)
+{
+    ReadJob *j = arg;
+    uint64_t done = 0;
+    while (done < j->len) {
+        const uint64_t want = j->len - done;
+        ssize_t r = pread(j->fd, j->dst + done, (size_t)(want > (1u << 30) ? (1u << 30) : want),
+                          (off_t)(j->off + done));
+        if (r <= 0) {
+            j->bad = 1;
+            return NULL;
+        }
+        done += (uint64_t)r;
+    }
+    return NULL;
+}
+
+/* The whole file into buf (readDecodedParticles, src/Gadget/BufVector3D.c:
+ * 285-308, reads it with one fread).  Files of 64 MB or more are read as
+ * contiguous stripes by several threads (positional reads), so copies out
+ * of the page cache or from a striped device proceed in parallel. */
 int sjcs_read_particles(const char *path, float *buf, uint64_t cap, uint64_t *n)
 {
-    uint64_t num, done = 0;
-    int fd;
+    uint64_t num;
+    int fd, T, t, bad = 0;
     if (sjcs_particle_file_count(path, &num) != 0)
         return -1;
     if (num > cap)
@@ -76,17 +104,36 @@ int sjcs_read_particles(const char *path, float *buf, uint64_t cap, uint64_t *n)
         return host_fail("ERROR: file %s not found in readDecodedParticles()", path);
     {
         const uint64_t total = num * 3 * sizeof(float);
-        char *dst = (char *)buf;
-        while (done < total) {
-            ssize_t r = read(fd, dst + done, (size_t)((total - done) > (1u << 30) ? (1u << 30) : (total - done)));
-            if (r <= 0) {
-                close(fd);
-                return host_fail("short read on %s", path);
-            }
-            done += (uint64_t)r;
+        ReadJob jobs[32];
+        pthread_t th[32];
+        int started[32] = {0};
+        T = total >= (64ull << 20) ? default_threads(0) : 1;
+        if (T > 16)
+            T = 16;
+        for (t = 0; t < T; ++t) {
+            /* stripes on 1 MB boundaries */
+            const uint64_t lo = (total * (uint64_t)t / (uint64_t)T) & ~((1ull << 20) - 1);
+            const uint64_t hi = (t == T - 1) ? total : (total * (uint64_t)(t + 1) / (uint64_t)T) & ~((1ull << 20) - 1);
+            jobs[t].fd = fd;
+            jobs[t].dst = (char *)buf + lo;
+            jobs[t].off = lo;
+            jobs[t].len = hi - lo;
+            jobs[t].bad = 0;
         }
+        for (t = 1; t < T; ++t)
+            started[t] = pthread_create(&th[t], NULL, read_job, &jobs[t]) == 0;
+        for (t = 0; t < T; ++t)
+            if (!started[t])
+                read_job(&jobs[t]); /* stripe 0, and any stripe whose thread did not start */
+        for (t = 1; t < T; ++t)
+            if (started[t])
+                pthread_join(th[t], NULL);
+        for (t = 0; t < T; ++t)
+            bad |= jobs[t].bad;
     }
     close(fd);
+    if (bad)
+        return host_fail("short read on %s", path);
     *n = num;
     return 0;
 }

@@ -218,15 +218,13 @@ static void start_index(sjcs_ctx *ctx, const char *fname, float radius_hint, Pen
         fprintf(stderr, "%s\n", sjcs_host_last_error());
         exit(EXIT_FAILURE);
     }
-    if (sjcs_host_alloc(n * 3 * sizeof(float), (void **)&p->host) != SJCS_OK)
-        die_lib("pinned buffer");
-    if (sjcs_read_particles(fname, p->host, n, &p->n) != 0) {
-        fprintf(stderr, "%s\n", sjcs_host_last_error());
-        exit(EXIT_FAILURE);
-    }
+    /* read in chunks through the context's staging slots, each chunk copied
+     * to the device as soon as it is read; the build is queued behind them */
+    p->host = NULL;
+    p->n = n;
+    if (sjcs_index_build_file(ctx, fname, &opts, &p->idx) != SJCS_OK)
+        die_lib("particle file read / index build");
     print_ms(">>>> particles reading time", t0);
-    if (sjcs_index_build(ctx, p->host, p->n, &opts, &p->idx) != SJCS_OK)
-        die_lib("index build");
 }
 
 static void finish_index(Pending *p, double t0)

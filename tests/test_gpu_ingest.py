@@ -1,0 +1,67 @@
+"""Particle file ingest (sjcs_index_build_file): chunked reads through the
+context's staging slots, each chunk uploaded as it is read.
+
+The index must be the one the host-buffer build makes from the same file
+(same counts), for files that end inside a chunk, span several chunks per
+reader thread, carry trailing bytes (count = file size / 12, as
+readDecodedParticles) or are empty; a missing file is refused.
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import oracle
+from spatialjoincountovershells_b200 import _native as nat
+
+pytestmark = pytest.mark.gpu
+
+CHUNK_PARTICLES = (16 << 20) / 12  # particles per staging chunk (not whole)
+
+
+def _counts(ctx, build, h, r2):
+    q = ctx.query(h, r2)
+    idx = build()
+    q.count(idx)
+    out = q.read_counts()
+    t = idx.timing()
+    idx.destroy()
+    q.destroy()
+    return out, t
+
+
+@pytest.mark.parametrize("n", [1, 5, 100_003, int(CHUNK_PARTICLES) + 1, 12_000_001])
+def test_file_build_matches_host_build(n, ctx, tmp_path):
+    rng = np.random.default_rng(n)
+    p = rng.uniform(0, 1000, size=(n, 3)).astype(np.float32)
+    h = rng.uniform(0, 1000, size=(2000, 3)).astype(np.float32)
+    r2 = nat.radius_table(0.01, 10, 24)
+    path = tmp_path / "part.dat"
+    nat.write_particle_file(path, p)
+    got, t = _counts(ctx, lambda: ctx.build_index_file(path, radius_hint=10), h, r2)
+    if n <= 100_003:
+        want = oracle.count(p, h, r2)
+    else:
+        want, _ = _counts(ctx, lambda: ctx.build_index(p, radius_hint=10), h, r2)
+    assert np.array_equal(got, want)
+    assert t["h2d_ms"] > 0
+
+
+def test_trailing_bytes_are_ignored_and_empty_files_build(ctx, tmp_path):
+    rng = np.random.default_rng(7)
+    p = rng.uniform(0, 1000, size=(5000, 3)).astype(np.float32)
+    h = rng.uniform(0, 1000, size=(300, 3)).astype(np.float32)
+    r2 = nat.radius_table(0.01, 30, 16)
+    path = tmp_path / "odd.dat"
+    path.write_bytes(p.tobytes() + b"\x01\x02\x03\x04\x05")  # 5 bytes past the last particle
+    got, _ = _counts(ctx, lambda: ctx.build_index_file(path, radius_hint=30), h, r2)
+    assert np.array_equal(got, oracle.count(p, h, r2))
+    empty = tmp_path / "empty.dat"
+    empty.write_bytes(b"")
+    got, _ = _counts(ctx, lambda: ctx.build_index_file(empty, radius_hint=30), h, r2)
+    assert not got.any()
+
+
+def test_missing_file_is_refused(ctx, tmp_path):
+    with pytest.raises(nat.SjcsError, match="not found"):
+        ctx.build_index_file(tmp_path / "nope.dat")
