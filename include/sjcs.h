@@ -203,7 +203,7 @@ int sjcs_index_build_device(sjcs_ctx *ctx, const float *d_xyz, uint64_t n,
                             const sjcs_index_opts *opts, sjcs_index **out);
 /* Same, reading a decoded particle file (x,y,z float triplets, count =
  * file size / 12, as readDecodedParticles, src/Gadget/BufVector3D.c:285-308).
- * Several threads read the file in 16 MB chunks into a small page-locked
+ * Several threads read the file in 8 MB chunks into a small page-locked
  * staging area owned by the context (allocated on first use) and each chunk is
  * copied to the device as soon as it is read, so no page-locked copy of the
  * whole file is made and reading overlaps the upload.  Returns once the file

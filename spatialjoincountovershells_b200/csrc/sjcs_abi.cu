@@ -631,7 +631,7 @@ int sjcs_index_build_device(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const
 }
 
 namespace {
-constexpr size_t kIngestChunk = 16u << 20;  // bytes per read and per copy
+constexpr size_t kIngestChunk = 8u << 20;  // bytes per read and per copy
 constexpr unsigned kIngestThreads = 8;      // reader threads = staging slots
 
 // Read [off, off + len) of fd completely.

@@ -16,7 +16,7 @@ from spatialjoincountovershells_b200 import _native as nat
 
 pytestmark = pytest.mark.gpu
 
-CHUNK_PARTICLES = (16 << 20) / 12  # particles per staging chunk (not whole)
+CHUNK_PARTICLES = (8 << 20) / 12  # particles per staging chunk (not whole)
 
 
 def _counts(ctx, build, h, r2):
