@@ -559,26 +559,25 @@ def time_steps(ctx, step, K, W, dist, local):
     ctx.sync()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     l0 = nat.launch_counter()
-    qs = []
+    cnt, calls = 0.0, 0
     with ClockSampler(local) as clk:
         e0.record(s_count)
         s_build.wait_event(e0)
         for _ in range(K):
             q = step()
             q.wait()
-            qs.append(q)
+            # read the count events and release the query at once, so the
+            # memory pool holds one step's queries, as in the warm-up
+            t = q.timing()
+            cnt += t["count_ms"]
+            calls += t["count_calls"]
+            q.destroy()
         e1.record(s_count)
         e1.synchronize()
     launches = nat.launch_counter() - l0
     ctx.sync()
     dist_barrier(dist, local)
     ms = dist_max(dist, e0.elapsed_time(e1) / K, local)
-    cnt, calls = 0.0, 0
-    for q in qs:
-        t = q.timing()
-        cnt += t["count_ms"]
-        calls += t["count_calls"]
-        q.destroy()
     return ms, int(launches), (cnt / calls if calls else None), clk.summary()
 
 

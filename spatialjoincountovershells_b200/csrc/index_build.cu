@@ -110,7 +110,7 @@ GridGeom auto_grid(uint64_t n, float radius_hint, const uint32_t* grid_req) {
             G[1] = (int)std::min(std::max(std::ceil(1000.0 / hyz), 1.0), 4096.0);
             G[2] = G[1];
             if ((double)G[0] * G[1] * G[2] <= kMaxCells) break;
-            hyz *= 1.01;  // rounding up per axis overshot the cap
+            hyz *= 1.002;  // rounding up per axis overshot the cap
         }
     }
     for (int a = 0; a < 3; ++a) {
