@@ -65,3 +65,40 @@ def test_trailing_bytes_are_ignored_and_empty_files_build(ctx, tmp_path):
 def test_missing_file_is_refused(ctx, tmp_path):
     with pytest.raises(nat.SjcsError, match="not found"):
         ctx.build_index_file(tmp_path / "nope.dat")
+
+
+def test_concurrent_file_builds_from_several_threads(ctx, tmp_path):
+    # host threads share the context's staging slots one file at a time; every
+    # index must still hold its own file
+    import threading
+    rng = np.random.default_rng(11)
+    files = []
+    for k in range(4):
+        p = rng.uniform(0, 1000, size=(2_000_000 + 777 * k, 3)).astype(np.float32)
+        path = tmp_path / f"part{k}.dat"
+        nat.write_particle_file(path, p)
+        files.append((path, p))
+    h = rng.uniform(0, 1000, size=(1500, 3)).astype(np.float32)
+    r2 = nat.radius_table(0.01, 12, 20)
+    built, errors = [None] * len(files), []
+
+    def work(k):
+        try:
+            built[k] = ctx.build_index_file(files[k][0], radius_hint=12)
+        except Exception as e:  # noqa: BLE001 - reported below
+            errors.append(e)
+
+    th = [threading.Thread(target=work, args=(k,)) for k in range(len(files))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join()
+    assert not errors
+    for k, (_, p) in enumerate(files):
+        q = ctx.query(h, r2)
+        q.count(built[k])
+        got = q.read_counts()
+        q.destroy()
+        built[k].destroy()
+        want, _ = _counts(ctx, lambda p=p: ctx.build_index(p, radius_hint=12), h, r2)
+        assert np.array_equal(got, want), k

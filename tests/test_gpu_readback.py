@@ -115,3 +115,23 @@ def test_pageable_memory_is_refused_and_empty_queries_pass(case, ctx):
     e.read_counts_async(np.zeros((0, NR), np.uint64))  # nothing to copy
     e.wait_read()
     e.destroy()
+
+
+def test_reads_of_two_queries_in_flight(case, ctx):
+    p1, p2, h, r2, c1, c2 = case
+    qa, qb = ctx.query(h, r2), ctx.query(h, r2)
+    i1 = ctx.build_index(p1, radius_hint=20)
+    i2 = ctx.build_index(p2, radius_hint=20)
+    qa.count(i1)
+    qb.count(i2)
+    a, b = _pinned(len(h)), _pinned(len(h))
+    qa.read_counts_async(a.array)
+    qb.read_counts_async(b.array)
+    qa.count(i2)  # waits on the device for qa's read only
+    qb.wait_read()
+    qa.wait_read()
+    assert np.array_equal(a.array, c1)
+    assert np.array_equal(b.array, c2)
+    assert np.array_equal(qa.read_counts(), c1 + c2)
+    for x in (i1, i2, qa, qb):
+        x.destroy()
