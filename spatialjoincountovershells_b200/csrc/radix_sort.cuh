@@ -76,14 +76,21 @@ k_radix_upsweep(KeyOp kop, uint64_t n, int shift, uint32_t* __restrict__ hist, u
     constexpr int BINS = RsDigit<BITS>::BINS;
     __shared__ uint32_t sh[RS_SUBHIST][BINS];
     const int tid = threadIdx.x;
+    const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
+    // keys first: their loads are in flight while the histograms are cleared
+    uint32_t key[RS_ITEMS];
+#pragma unroll
+    for (int i = 0; i < RS_ITEMS; ++i) {
+        const uint64_t idx = base + (uint64_t)i * RS_THREADS + tid;
+        key[i] = idx < n ? kop(idx) : 0u;
+    }
     for (int i = tid; i < RS_SUBHIST * BINS; i += RS_THREADS) (&sh[0][0])[i] = 0;
     __syncthreads();
-    const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
     uint32_t* mine = sh[(tid >> 5) % RS_SUBHIST];
 #pragma unroll
     for (int i = 0; i < RS_ITEMS; ++i) {
         const uint64_t idx = base + (uint64_t)i * RS_THREADS + tid;
-        if (idx < n) atomicAdd(&mine[(kop(idx) >> shift) & (BINS - 1)], 1u);
+        if (idx < n) atomicAdd(&mine[(key[i] >> shift) & (BINS - 1)], 1u);
     }
     __syncthreads();
     for (int d = tid; d < BINS; d += RS_THREADS) {
