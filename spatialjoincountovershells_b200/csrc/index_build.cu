@@ -53,28 +53,54 @@ struct Gap {
 };
 constexpr uint32_t kGapInline = 64;
 
-// cell_start[c] = i for every cell c in (key[i-1], key[i]] (key[-1] = -1,
-// key[n] = ncells), so empty cells point at the next occupied slot and
-// cell_start[ncells] = n.  Long runs of empty cells go to a gap list that a
-// second kernel fills cooperatively.
-__global__ void k_cell_start(const uint32_t* __restrict__ keys, uint64_t n, uint64_t ncells,
-                             uint32_t* __restrict__ cs, Gap* __restrict__ gaps,
-                             uint32_t* __restrict__ ngaps, uint32_t max_gaps) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > n) return;
-    const uint64_t lo = (i == 0) ? 0ull : (uint64_t)keys[i - 1] + 1ull;
-    const uint64_t hi = (i == n) ? ncells : (uint64_t)keys[i];
+// cell_start[c] = i for every cell c in [lo, hi] (lo > hi: nothing); runs
+// longer than kGapInline go to the gap list.
+__device__ __forceinline__ void fill_cells(uint64_t lo, uint64_t hi, uint32_t i, uint32_t* __restrict__ cs,
+                                           Gap* __restrict__ gaps, uint32_t* __restrict__ ngaps,
+                                           uint32_t max_gaps) {
     if (lo > hi) return;
     const uint64_t cnt = hi - lo + 1;
     const uint64_t inl = cnt < kGapInline ? cnt : kGapInline;
-    for (uint64_t c = 0; c < inl; ++c) cs[lo + c] = (uint32_t)i;
+    for (uint64_t c = 0; c < inl; ++c) cs[lo + c] = i;
     if (cnt > kGapInline) {
         const uint32_t slot = atomicAdd(ngaps, 1u);
         if (slot < max_gaps) {
-            gaps[slot] = Gap{(uint32_t)(lo + kGapInline), (uint32_t)hi, (uint32_t)i};
+            gaps[slot] = Gap{(uint32_t)(lo + kGapInline), (uint32_t)hi, i};
         } else {
-            for (uint64_t c = lo + kGapInline; c <= hi; ++c) cs[c] = (uint32_t)i;
+            for (uint64_t c = lo + kGapInline; c <= hi; ++c) cs[c] = i;
         }
+    }
+}
+
+// cell_start[c] = i for every cell c in (key[i-1], key[i]] (key[-1] = -1,
+// key[n] = ncells), so empty cells point at the next occupied slot and
+// cell_start[ncells] = n.  Thread t takes boundaries i = 4t .. 4t+3, reading
+// their keys with one 16-byte load when the key array is 16-byte aligned.
+// Long runs of empty cells go to a gap list that a second kernel fills
+// cooperatively.
+__global__ void k_cell_start(const uint32_t* __restrict__ keys, uint64_t n, uint64_t ncells,
+                             uint32_t* __restrict__ cs, Gap* __restrict__ gaps,
+                             uint32_t* __restrict__ ngaps, uint32_t max_gaps, int vec) {
+    const uint64_t i0 = 4 * ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x);
+    if (i0 > n) return;
+    uint64_t cur[4];
+    if (vec && i0 + 4 <= n) {
+        const uint4 v = *reinterpret_cast<const uint4*>(keys + i0);
+        cur[0] = v.x;
+        cur[1] = v.y;
+        cur[2] = v.z;
+        cur[3] = v.w;
+    } else {
+#pragma unroll
+        for (int j = 0; j < 4; ++j) cur[j] = (i0 + j < n) ? (uint64_t)keys[i0 + j] : ncells;
+    }
+    uint64_t lo = (i0 == 0) ? 0ull : (uint64_t)keys[i0 - 1] + 1ull;
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const uint64_t i = i0 + (uint64_t)j;
+        if (i > n) break;
+        fill_cells(lo, cur[j], (uint32_t)i, cs, gaps, ngaps, max_gaps);
+        lo = cur[j] + 1ull;
     }
 }
 
@@ -159,10 +185,11 @@ int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const Gri
 int fill_cell_table(const uint32_t* sorted_cells, uint64_t n, uint64_t ncells, uint32_t* cell_start, void* gaps,
                     uint32_t* ngaps, cudaStream_t s) {
     SJCS_CUDA_TRY(cudaMemsetAsync(ngaps, 0, sizeof(uint32_t), s));
-    const uint64_t threads = n + 1;
+    const uint64_t threads = n / 4 + 1;  // boundaries 0..n, four per thread
     const unsigned blocks = (unsigned)((threads + 255) / 256);
+    const int vec = (reinterpret_cast<uintptr_t>(sorted_cells) & 15u) == 0;
     k_cell_start<<<blocks, 256, 0, s>>>(sorted_cells, n, ncells, cell_start, static_cast<Gap*>(gaps), ngaps,
-                                        kGridGaps);
+                                        kGridGaps, vec);
     SJCS_LAUNCH_CHECK();
     k_fill_gaps<<<1024, 256, 0, s>>>(static_cast<Gap*>(gaps), ngaps, kGridGaps, cell_start);
     SJCS_LAUNCH_CHECK();

@@ -70,28 +70,20 @@ struct SinkRecords {
     }
 };
 
-template <int BITS, class KeyOp>
-__global__ void __launch_bounds__(RS_THREADS)
-k_radix_upsweep(KeyOp kop, uint64_t n, int shift, uint32_t* __restrict__ hist, uint32_t ntiles) {
+// Digit histogram of one tile from the keys a thread holds (item i counted
+// when bit i of `valid` is set) -> hist[digit][tile].
+template <int BITS>
+__device__ __forceinline__ void tile_histogram(const uint32_t (&key)[RS_ITEMS], uint32_t valid, int shift,
+                                               uint32_t* __restrict__ hist, uint32_t ntiles) {
     constexpr int BINS = RsDigit<BITS>::BINS;
     __shared__ uint32_t sh[RS_SUBHIST][BINS];
     const int tid = threadIdx.x;
-    const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
-    // keys first: their loads are in flight while the histograms are cleared
-    uint32_t key[RS_ITEMS];
-#pragma unroll
-    for (int i = 0; i < RS_ITEMS; ++i) {
-        const uint64_t idx = base + (uint64_t)i * RS_THREADS + tid;
-        key[i] = idx < n ? kop(idx) : 0u;
-    }
     for (int i = tid; i < RS_SUBHIST * BINS; i += RS_THREADS) (&sh[0][0])[i] = 0;
     __syncthreads();
     uint32_t* mine = sh[(tid >> 5) % RS_SUBHIST];
 #pragma unroll
-    for (int i = 0; i < RS_ITEMS; ++i) {
-        const uint64_t idx = base + (uint64_t)i * RS_THREADS + tid;
-        if (idx < n) atomicAdd(&mine[(key[i] >> shift) & (BINS - 1)], 1u);
-    }
+    for (int i = 0; i < RS_ITEMS; ++i)
+        if (valid & (1u << i)) atomicAdd(&mine[(key[i] >> shift) & (BINS - 1)], 1u);
     __syncthreads();
     for (int d = tid; d < BINS; d += RS_THREADS) {
         uint32_t s = 0;
@@ -99,6 +91,22 @@ k_radix_upsweep(KeyOp kop, uint64_t n, int shift, uint32_t* __restrict__ hist, u
         for (int h = 0; h < RS_SUBHIST; ++h) s += sh[h][d];
         hist[(uint64_t)d * ntiles + blockIdx.x] = s;
     }
+}
+
+template <int BITS, class KeyOp>
+__global__ void __launch_bounds__(RS_THREADS)
+k_radix_upsweep(KeyOp kop, uint64_t n, int shift, uint32_t* __restrict__ hist, uint32_t ntiles) {
+    const int tid = threadIdx.x;
+    const uint64_t base = (uint64_t)blockIdx.x * RS_TILE;
+    // keys first: their loads are in flight while the histograms are cleared
+    uint32_t key[RS_ITEMS], valid = 0;
+#pragma unroll
+    for (int i = 0; i < RS_ITEMS; ++i) {
+        const uint64_t idx = base + (uint64_t)i * RS_THREADS + tid;
+        key[i] = idx < n ? kop(idx) : 0u;
+        valid |= (idx < n ? 1u : 0u) << i;
+    }
+    tile_histogram<BITS>(key, valid, shift, hist, ntiles);
 }
 
 // 16-byte asynchronous global -> shared copy (cp.async, L2 only); the copies
@@ -139,6 +147,39 @@ template <>
 struct PayIsXyz<PayFromXyzStaged> {
     static constexpr bool value = true;
 };
+
+// First-pass histogram over a 16-byte-aligned (x, y, z) float array: thread t
+// of a tile takes its 8 consecutive particles as six 16-byte loads (96 bytes,
+// 16-byte aligned because a tile starts at a multiple of 4096 particles) and
+// computes their keys with KeyOp::key_of.  Which thread counts which particle
+// does not matter to a histogram.
+template <int BITS, class KeyOp>
+__global__ void __launch_bounds__(RS_THREADS)
+k_radix_upsweep_xyz(KeyOp kop, const float* __restrict__ xyz, uint64_t n, int shift, uint32_t* __restrict__ hist,
+                    uint32_t ntiles) {
+    static_assert(RS_ITEMS == 8, "six float4 per thread hold 8 particles");
+    const int tid = threadIdx.x;
+    const uint64_t p0 = (uint64_t)blockIdx.x * RS_TILE + (uint64_t)tid * RS_ITEMS;
+    uint32_t key[RS_ITEMS], valid = 0;
+    if (p0 + RS_ITEMS <= n) {
+        const float4* v = reinterpret_cast<const float4*>(xyz + 3 * p0);
+        float4 a[6];
+#pragma unroll
+        for (int j = 0; j < 6; ++j) a[j] = __ldg(v + j);
+        const float* f = reinterpret_cast<const float*>(a);
+#pragma unroll
+        for (int i = 0; i < RS_ITEMS; ++i) key[i] = kop.key_of(f[3 * i], f[3 * i + 1], f[3 * i + 2]);
+        valid = 0xffu;
+    } else {
+#pragma unroll
+        for (int i = 0; i < RS_ITEMS; ++i) {
+            const uint64_t p = p0 + (uint64_t)i;
+            key[i] = p < n ? kop.key_of(xyz[3 * p], xyz[3 * p + 1], xyz[3 * p + 2]) : 0u;
+            valid |= (p < n ? 1u : 0u) << i;
+        }
+    }
+    tile_histogram<BITS>(key, valid, shift, hist, ntiles);
+}
 
 template <int BITS, class KeyOp, class PayOp, class Sink>
 __global__ void __launch_bounds__(RS_THREADS)
@@ -288,7 +329,10 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
 template <int BITS = RS_BITS, class KeyOp, class PayOp, class Sink>
 int radix_pass(KeyOp kop, PayOp pop, Sink sink, uint64_t n, int shift, uint32_t* hist, uint32_t ntiles,
                cudaStream_t s, uint32_t* partials) {
-    k_radix_upsweep<BITS><<<ntiles, RS_THREADS, 0, s>>>(kop, n, shift, hist, ntiles);
+    if constexpr (PayIsXyz<PayOp>::value)
+        k_radix_upsweep_xyz<BITS><<<ntiles, RS_THREADS, 0, s>>>(kop, pop.xyz, n, shift, hist, ntiles);
+    else
+        k_radix_upsweep<BITS><<<ntiles, RS_THREADS, 0, s>>>(kop, n, shift, hist, ntiles);
     SJCS_LAUNCH_CHECK();
     int rc = exclusive_scan_u32(hist, (uint64_t)RsDigit<BITS>::BINS * ntiles, s, partials);
     if (rc) return rc;
