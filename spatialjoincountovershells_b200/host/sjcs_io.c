@@ -581,9 +581,10 @@ int sjcs_write_result(const char *path, const sjcs_halo *halos, uint64_t nhalos,
     float *rad = NULL;
     uint64_t *total = NULL, h;
     int i, T, rc = -1;
-    FmtJob *jobs = NULL;
+    FmtJob *jobs = NULL; /* two rounds of T jobs: one is written while the other is formatted */
     pthread_t *th = NULL;
-    const uint64_t per_job = 16384;
+    int *started = NULL;
+    const uint64_t per_job = 8192;
 
     if (nrads <= 0 || !r2)
         return host_fail("invalid radius table");
@@ -623,39 +624,52 @@ int sjcs_write_result(const char *path, const sjcs_halo *halos, uint64_t nhalos,
         goto out;
     }
     T = default_threads(nthreads);
-    jobs = calloc(T, sizeof(FmtJob));
-    th = calloc(T, sizeof(pthread_t));
-    if (!jobs || !th)
+    jobs = calloc(2 * (size_t)T, sizeof(FmtJob));
+    th = calloc(2 * (size_t)T, sizeof(pthread_t));
+    started = calloc(2 * (size_t)T, sizeof(int));
+    if (!jobs || !th || !started)
         goto close_out;
-    for (i = 0; i < T; ++i) {
+    for (i = 0; i < 2 * T; ++i) {
         jobs[i].buf = malloc(per_job * (24 + (size_t)nrads * (maxline + 22)));
         if (!jobs[i].buf)
             goto close_out;
     }
-    for (h = 0; h < nhalos;) {
-        int used = 0;
-        for (i = 0; i < T && h < nhalos; ++i) {
-            uint64_t e = h + per_job < nhalos ? h + per_job : nhalos;
-            jobs[i].halos = halos;
-            jobs[i].counts = counts;
-            jobs[i].lo = h;
-            jobs[i].hi = e;
-            jobs[i].nrads = nrads;
-            jobs[i].labels = labels;
-            jobs[i].label_len = label_len;
-            h = e;
-            used++;
-        }
-        for (i = 1; i < used; ++i)
-            pthread_create(&th[i], NULL, fmt_job, &jobs[i]);
-        fmt_job(&jobs[0]);
-        for (i = 1; i < used; ++i)
-            pthread_join(th[i], NULL);
-        for (i = 0; i < used; ++i) {
-            if (fwrite(jobs[i].buf, 1, jobs[i].len, fp) != jobs[i].len) {
+    /* Round r is formatted by threads into job set r % 2 while this thread
+     * writes round r - 1 from the other set, in halo order. */
+    {
+        int prev_used = 0, r = 0, werr = 0;
+        for (h = 0; h < nhalos || prev_used; ++r) {
+            FmtJob *cur = jobs + (size_t)(r & 1) * T, *prev = jobs + (size_t)((r + 1) & 1) * T;
+            pthread_t *cth = th + (size_t)(r & 1) * T;
+            int *cst = started + (size_t)(r & 1) * T;
+            int used = 0;
+            for (i = 0; i < T && h < nhalos; ++i) {
+                uint64_t e = h + per_job < nhalos ? h + per_job : nhalos;
+                cur[i].halos = halos;
+                cur[i].counts = counts;
+                cur[i].lo = h;
+                cur[i].hi = e;
+                cur[i].nrads = nrads;
+                cur[i].labels = labels;
+                cur[i].label_len = label_len;
+                h = e;
+                used++;
+            }
+            for (i = 0; i < used; ++i)
+                cst[i] = pthread_create(&cth[i], NULL, fmt_job, &cur[i]) == 0;
+            for (i = 0; i < prev_used && !werr; ++i)
+                werr = fwrite(prev[i].buf, 1, prev[i].len, fp) != prev[i].len;
+            for (i = 0; i < used; ++i) {
+                if (cst[i])
+                    pthread_join(cth[i], NULL);
+                else
+                    fmt_job(&cur[i]); /* no thread: format it here */
+            }
+            if (werr) {
                 host_fail("ERROR: while writing %s in outputResult()", path ? path : "(stdout)");
                 goto close_out;
             }
+            prev_used = used;
         }
     }
     fputs("\nTotal\n", fp);
@@ -679,10 +693,11 @@ close_out:
         fflush(stdout);
 out:
     if (jobs)
-        for (i = 0; i < T; ++i)
+        for (i = 0; i < 2 * T; ++i)
             free(jobs[i].buf);
     free(jobs);
     free(th);
+    free(started);
     if (labels)
         for (i = 0; i < nrads; ++i)
             free(labels[i]);
