@@ -549,6 +549,35 @@ typedef struct FmtJob {
     size_t len;
 } FmtJob;
 
+static size_t dec_len(uint64_t v)
+{
+    size_t k = 1;
+    while (v >= 10) {
+        v /= 10;
+        ++k;
+    }
+    return k;
+}
+
+/* Bytes fmt_job writes for halos [lo, hi) (into j->len). */
+static void *len_job(void *arg)
+{
+    FmtJob *j = arg;
+    uint64_t h;
+    size_t len = 0, labels = 0;
+    int i;
+    for (i = 0; i < j->nrads; ++i)
+        labels += j->label_len[i] + 1;
+    for (h = j->lo; h < j->hi; ++h) {
+        const uint64_t *c = j->counts + h * (uint64_t)j->nrads;
+        len += 4 + dec_len(j->halos[h].id) + labels;
+        for (i = 0; i < j->nrads; ++i)
+            len += dec_len(c[i]);
+    }
+    j->len = len;
+    return NULL;
+}
+
 static void *fmt_job(void *arg)
 {
     FmtJob *j = arg;
@@ -570,6 +599,117 @@ static void *fmt_job(void *arg)
     }
     j->len = (size_t)(o - j->buf);
     return NULL;
+}
+
+/* Run fn over jobs[0..n) on threads (inline where a thread cannot start). */
+static void run_jobs(void *(*fn)(void *), FmtJob *jobs, int n, pthread_t *th, int *started)
+{
+    int t;
+    for (t = 1; t < n; ++t)
+        started[t] = pthread_create(&th[t], NULL, fn, &jobs[t]) == 0;
+    started[0] = 0;
+    for (t = 0; t < n; ++t)
+        if (!started[t])
+            fn(&jobs[t]);
+    for (t = 1; t < n; ++t)
+        if (started[t])
+            pthread_join(th[t], NULL);
+}
+
+/* Mapped writer for regular files: the exact size is computed first (one
+ * parallel pass over the counts), the file's blocks are allocated up front
+ * (so running out of space is an error here, never a fault while writing the
+ * mapping), and every thread formats its halos straight into a shared mapping
+ * at its own offset: no single writer to wait for.  Returns 0 = written,
+ * -1 = failed (error set), 1 = use the stream writer (not a regular file, or
+ * the file system cannot preallocate or map it). */
+static int write_result_mapped(const char *path, const sjcs_halo *halos, uint64_t nhalos, const uint64_t *counts,
+                               int nrads, char **labels, size_t *label_len, const uint64_t *total, int T)
+{
+    struct stat st;
+    int fd, t, njobs, rc = -1;
+    FmtJob *jobs = NULL;
+    pthread_t *th = NULL;
+    int *started = NULL;
+    size_t maxline = 0, tail_len = 0, body = 0, size;
+    char *tail = NULL, *map;
+    uint64_t off;
+    if (stat(path, &st) == 0 && !S_ISREG(st.st_mode))
+        return 1;
+    for (t = 0; t < nrads; ++t)
+        if (label_len[t] > maxline)
+            maxline = label_len[t];
+    njobs = T * 4;
+    if ((uint64_t)njobs > nhalos)
+        njobs = nhalos ? (int)nhalos : 1;
+    jobs = calloc((size_t)njobs, sizeof(FmtJob));
+    th = calloc((size_t)njobs, sizeof(pthread_t));
+    started = calloc((size_t)njobs, sizeof(int));
+    tail = malloc(8 + (size_t)nrads * (maxline + 22));
+    if (!jobs || !th || !started || !tail) {
+        host_fail("ERROR: memory shortage in outputResult()");
+        goto out;
+    }
+    for (t = 0; t < njobs; ++t) {
+        jobs[t].halos = halos;
+        jobs[t].counts = counts;
+        jobs[t].lo = nhalos * (uint64_t)t / (uint64_t)njobs;
+        jobs[t].hi = nhalos * (uint64_t)(t + 1) / (uint64_t)njobs;
+        jobs[t].nrads = nrads;
+        jobs[t].labels = labels;
+        jobs[t].label_len = label_len;
+    }
+    run_jobs(len_job, jobs, njobs, th, started);
+    for (t = 0; t < njobs; ++t)
+        body += jobs[t].len;
+    /* the Total block: the running total is halo 0's own row (main.c:400, 413) */
+    memcpy(tail, "\nTotal\n", 7);
+    tail_len = 7;
+    for (t = 0; t < nrads; ++t) {
+        memcpy(tail + tail_len, labels[t], label_len[t]);
+        tail_len += label_len[t];
+        tail_len += put_u64(tail + tail_len, total[t]);
+        tail[tail_len++] = '\n';
+    }
+    size = body + tail_len;
+    fd = open(path, O_RDWR | O_CREAT | O_TRUNC, 0666);
+    if (fd < 0) {
+        host_fail("Cannot create %s in outputResult().", path);
+        goto out;
+    }
+    if (fallocate(fd, 0, 0, (off_t)size) != 0) {
+        const int e = errno;
+        close(fd);
+        if (e == ENOSPC || e == EFBIG || e == EDQUOT)
+            host_fail("ERROR: while writing %s in outputResult()", path);
+        else
+            rc = 1;
+        goto out;
+    }
+    map = mmap(NULL, size, PROT_READ | PROT_WRITE, MAP_SHARED, fd, 0);
+    if (map == MAP_FAILED) {
+        close(fd);
+        rc = 1;
+        goto out;
+    }
+    off = 0;
+    for (t = 0; t < njobs; ++t) {
+        jobs[t].buf = map + off;
+        off += jobs[t].len;
+    }
+    run_jobs(fmt_job, jobs, njobs, th, started);
+    memcpy(map + body, tail, tail_len);
+    rc = 0;
+    if (munmap(map, size) != 0)
+        rc = host_fail("ERROR: while writing %s in outputResult()", path);
+    if (close(fd) != 0 && rc == 0)
+        rc = host_fail("ERROR: while writing %s in outputResult()", path);
+out:
+    free(jobs);
+    free(th);
+    free(started);
+    free(tail);
+    return rc;
 }
 
 int sjcs_write_result(const char *path, const sjcs_halo *halos, uint64_t nhalos, const float *r2, int nrads,
@@ -618,6 +758,14 @@ int sjcs_write_result(const char *path, const sjcs_halo *halos, uint64_t nhalos,
         for (i = 0; i < nrads; ++i)
             total[i] += counts[i];
 
+    if (path) {
+        const int m = write_result_mapped(path, halos, nhalos, counts, nrads, labels, label_len, total,
+                                          default_threads(nthreads));
+        if (m <= 0) {
+            rc = m;
+            goto out;
+        }
+    }
     fp = path ? fopen(path, "w") : stdout;
     if (!fp) {
         host_fail("Cannot create %s in outputResult().", path);
