@@ -125,11 +125,12 @@ GridGeom auto_grid(uint64_t n, float radius_hint, const uint32_t* grid_req) {
         // can be finer than y/z for free: cells are 2.5x longer in y and z.
         // Target about 1.6 cells per particle, at most 2^27 cells (a 27-bit
         // cell key sorts in three 9-bit radix passes), and keep y/z cells
-        // >= R/2 so a query box spans at most 5x5 rows.
+        // >= R/4: a query box then spans at most 9x9 rows (boxes of more
+        // than 25 rows are counted without the per-batch row plan).
         constexpr double kMaxCells = 134217728.0;  // 2^27
         const double target = std::min(std::max(1.6 * (double)n, 4096.0), kMaxCells);
         double hyz = std::cbrt(2.5e9 / target);
-        if (radius_hint > 0.0f) hyz = std::max(hyz, 0.5 * (double)radius_hint);
+        if (radius_hint > 0.0f) hyz = std::max(hyz, 0.25 * (double)radius_hint);
         for (;;) {
             const double hx = hyz / 2.5;
             G[0] = (int)std::min(std::max(std::ceil(1000.0 / hx), 1.0), 4096.0);

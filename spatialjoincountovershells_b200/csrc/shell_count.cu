@@ -185,7 +185,7 @@ struct HaloPlan {
 };
 constexpr uint32_t kSlowPlan = 0xffffffffu;
 constexpr int kBatch = 32;    // halos per warp batch (one per lane while planning)
-constexpr int kMaxRows = 25;  // rows kept per halo (a box spans <= 5x5 rows when cells are >= R/2)
+constexpr int kMaxRows = 25;  // rows kept per halo (5x5 rows: boxes up to 2R <= 4 y/z cells)
 
 // Shared memory of one warp: plans and row lists of its current batch (24 B
 // plans and 25-row lists keep a block at ~25 KB, so 8 blocks fit an SM).
