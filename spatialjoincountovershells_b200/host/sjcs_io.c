@@ -157,30 +157,128 @@ int sjcs_write_particle_file(const char *path, const float *xyz, uint64_t n)
 /* GetDataFromLineFast, src/Gadget/BufHalo.c:218-249: id = strtoul of the
  * line, mass after the 2nd space, x after 6 more spaces, y and z after one
  * more each.  str is NUL-terminated like the reference's fgets buffer. */
+/* Fast exact forms of strtof / strtoul for the plain decimal tokens the halo
+ * files hold ("123.456789", "-0.5", "42"); anything else -- leading blanks,
+ * exponents, hex, inf/nan, more than 19 significant digits, a value whose
+ * conversion cannot be proven correctly rounded -- returns 0 and the caller
+ * uses the C library, so the result always equals strtof's / strtoul's.
+ *
+ * A token is [-+]digits[.digits] ending at a character that cannot continue
+ * a number.  Its value is m / 10^k exactly.  With m < 2^24 and k <= 10 both
+ * are floats, and one float division is correctly rounded (Clinger).  With
+ * m < 2^53 and k <= 22 both are doubles, the double quotient q is correctly
+ * rounded, and rounding q to float equals rounding m / 10^k to float unless
+ * q lies exactly on a midpoint between two floats (rounding is monotone and
+ * every such midpoint is a double, so q can reach the other side of one only
+ * by landing on it); q near a midpoint therefore goes to strtof. */
+static const float kPow10f[11] = {1e0f, 1e1f, 1e2f, 1e3f, 1e4f, 1e5f, 1e6f, 1e7f, 1e8f, 1e9f, 1e10f};
+static const double kPow10d[23] = {1e0,  1e1,  1e2,  1e3,  1e4,  1e5,  1e6,  1e7,  1e8,  1e9,  1e10, 1e11,
+                                   1e12, 1e13, 1e14, 1e15, 1e16, 1e17, 1e18, 1e19, 1e20, 1e21, 1e22};
+
+static int continues_number(char c)
+{
+    return (c >= '0' && c <= '9') || c == '.' || (c >= 'a' && c <= 'z') || (c >= 'A' && c <= 'Z');
+}
+
+static int fast_f32(const char *s, float *out)
+{
+    int neg = 0, digits = 0, k = 0;
+    uint64_t m = 0;
+    if (*s == '-' || *s == '+')
+        neg = (*s++ == '-');
+    if (*s < '0' || *s > '9')
+        return 0;
+    while (*s >= '0' && *s <= '9') {
+        if (m || *s != '0')
+            ++digits;
+        m = m * 10u + (uint64_t)(*s++ - '0');
+        if (digits > 19)
+            return 0;
+    }
+    if (*s == '.') {
+        ++s;
+        while (*s >= '0' && *s <= '9') {
+            if (m || *s != '0')
+                ++digits;
+            m = m * 10u + (uint64_t)(*s++ - '0');
+            ++k;
+            if (digits > 19 || k > 22)
+                return 0;
+        }
+    }
+    if (continues_number(*s))
+        return 0;
+    if (m < (1u << 24) && k <= 10) {
+        const float v = (float)m / kPow10f[k];
+        *out = neg ? -v : v;
+        return 1;
+    }
+    if (m < (1ull << 53)) {
+        const double q = (double)m / kPow10d[k];
+        uint64_t bits;
+        memcpy(&bits, &q, sizeof(bits));
+        {
+            const int e = (int)((bits >> 52) & 0x7ff) - 1023;
+            const uint32_t excess = (uint32_t)(bits & 0x1fffffffu); /* double bits below a float's */
+            if (q == 0.0 || e < -126 || e > 127)
+                return 0;
+            if (excess >= 0x0ffffffeu && excess <= 0x10000002u)
+                return 0; /* at or next to a midpoint */
+        }
+        *out = neg ? -(float)q : (float)q;
+        return 1;
+    }
+    return 0;
+}
+
+static int fast_u64(const char *s, unsigned long *out)
+{
+    uint64_t m = 0;
+    int n = 0;
+    if (*s < '0' || *s > '9')
+        return 0;
+    while (*s >= '0' && *s <= '9') {
+        m = m * 10u + (uint64_t)(*s++ - '0');
+        if (++n > 19)
+            return 0;
+    }
+    *out = (unsigned long)m;
+    return 1;
+}
+
+static float f32_token(const char *s)
+{
+    float v;
+    return fast_f32(s, &v) ? v : strtof(s, NULL);
+}
+
 static int parse_record(char *str, sjcs_halo *h)
 {
     int i;
-    h->id = strtoul(str, NULL, 10);
+    {
+        unsigned long id;
+        h->id = fast_u64(str, &id) ? id : strtoul(str, NULL, 10);
+    }
     for (i = 0; i < 2; i++) {
         if ((str = strchr(str, ' ')) == NULL)
             return -1;
         str++;
     }
-    h->mass = strtof(str, NULL);
+    h->mass = f32_token(str);
     for (i = 0; i < 6; i++) {
         if ((str = strchr(str, ' ')) == NULL)
             return -1;
         str++;
     }
-    h->point[0] = strtof(str, NULL);
+    h->point[0] = f32_token(str);
     if ((str = strchr(str, ' ')) == NULL)
         return -1;
     str++;
-    h->point[1] = strtof(str, NULL);
+    h->point[1] = f32_token(str);
     if ((str = strchr(str, ' ')) == NULL)
         return -1;
     str++;
-    h->point[2] = strtof(str, NULL);
+    h->point[2] = f32_token(str);
     return 0;
 }
 

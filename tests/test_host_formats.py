@@ -146,3 +146,52 @@ def test_result_writer_reproduces_reference_text(name, case_dirs, manifest, tmp_
     assert hashlib.sha256(data).hexdigest() == manifest[name]["sha256"]
     if name == "kat":
         assert data == (cases.pathlib.Path(__file__).parent / "golden" / "kat_result.txt").read_bytes()
+
+
+def _libc_strtof():
+    import ctypes
+    libc = ctypes.CDLL(None)
+    f = libc.strtof
+    f.restype = ctypes.c_float
+    f.argtypes = [ctypes.c_char_p, ctypes.c_void_p]
+    return f
+
+
+def test_halo_reader_floats_equal_strtof(tmp_path, built):
+    # The reader converts the plain decimal tokens itself and hands everything
+    # else to strtof; either way each value must be strtof's, bit for bit.
+    # Tokens: random widths and signs, exponents, hex, inf/nan, 20+ digits,
+    # and shortest double representations of float midpoints (whose double
+    # conversion lands exactly on the midpoint while their exact value is
+    # just beside it).
+    rng = np.random.default_rng(12)
+    toks = []
+    for _ in range(6000):
+        ip = str(rng.integers(0, 10 ** rng.integers(1, 12)))
+        fp = "".join(rng.choice(list("0123456789"), size=rng.integers(0, 14)))
+        t = ip + ("." + fp if rng.random() < 0.9 else "")
+        toks.append(("-" if rng.random() < 0.2 else "") + t)
+    f32 = rng.uniform(0.0, 1000.0, 6000).astype(np.float32)
+    nxt = np.nextafter(f32, np.float32(np.inf))
+    for a, b in zip(f32.astype(np.float64), nxt.astype(np.float64)):
+        toks.append(repr((a + b) / 2.0))  # exact midpoint as a double, shortest round-trip digits
+    # 16 significant digits (< 2^53 as an integer): their double conversion
+    # is often exactly the float midpoint they approximate
+    f32 = rng.uniform(1.0, 9.0, 6000).astype(np.float32)
+    nxt = np.nextafter(f32, np.float32(np.inf))
+    for a, b in zip(f32.astype(np.float64), nxt.astype(np.float64)):
+        toks.append("%.15f" % ((a + b) / 2.0))
+    toks += ["0", "-0", "+3.5", "1e3", "2.5E-1", "0x1p3", "inf", "-nan", "1.", "007.250",
+             "12345678901234567890.5", "0.0000000000000000000001", "340282356779733661637539395458142568448",
+             "16777217", "16777217.0", "9007199254740993", "1.00000005960464477539062500001"]
+    lines = [f"{i + 1} 0 {t} 0 0 0 0 0 {t} {toks[-1 - (i % len(toks))]} 1.5\n" for i, t in enumerate(toks)]
+    f = tmp_path / "h.list"
+    f.write_text(_halo_text(lines))
+    h = nat.read_halos(f, nthreads=1)
+    strtof = _libc_strtof()
+    want = np.array([strtof(t.encode(), None) for t in toks], np.float32)
+    want_y = np.array([strtof(toks[-1 - (i % len(toks))].encode(), None) for i in range(len(toks))], np.float32)
+    assert np.array_equal(h["mass"].view(np.uint32), want.view(np.uint32))
+    assert np.array_equal(h["point"][:, 0].view(np.uint32), want.view(np.uint32))
+    assert np.array_equal(h["point"][:, 1].view(np.uint32), want_y.view(np.uint32))
+    assert np.array_equal(h["id"], np.arange(1, len(toks) + 1, dtype=np.uint64))
