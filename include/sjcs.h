@@ -210,6 +210,13 @@ int sjcs_index_build_device(sjcs_ctx *ctx, const float *d_xyz, uint64_t n,
  * is read and the copies and the build are queued.  A missing or unreadable
  * file fails with SJCS_ERR_INVALID. */
 int sjcs_index_build_file(sjcs_ctx *ctx, const char *path, const sjcs_index_opts *opts, sjcs_index **out);
+/* Get a context ready for particle files of up to max_particles: page-lock
+ * the staging slots of sjcs_index_build_file and grow the device pool to hold
+ * one file's upload, index and build scratch, so the first file pays for
+ * neither.  It may run on a helper thread while the caller does host work
+ * that does not use the context (the driver parses the halo file meanwhile).
+ * No counterpart in the reference (its buffers are allocated per file). */
+int sjcs_ctx_prepare_files(sjcs_ctx *ctx, uint64_t max_particles);
 /* Same, from compressed (Gadget-encoded) particles: n uint16 triplets in HOST
  * memory (the displacement record of a compressed file) and the file's
  * 256-byte header (the layout of GadgetHeader, include/Gadget/GadgetHeader.h:4-27;

@@ -128,6 +128,7 @@ _SIGS = {
     "sjcs_query_count": (_c.c_int, [_vp, _vp, _vp]),
     "sjcs_query_wait": (_c.c_int, [_vp]),
     "sjcs_index_build_file": (_c.c_int, [_vp, _c.c_char_p, _c.POINTER(sjcs_index_opts), _pp]),
+    "sjcs_ctx_prepare_files": (_c.c_int, [_vp, _u64]),
     "sjcs_query_read_counts": (_c.c_int, [_vp, _vp, _vp, _c.c_int]),
     "sjcs_query_read_counts_async": (_c.c_int, [_vp, _vp, _vp]),
     "sjcs_query_wait_read": (_c.c_int, [_vp]),
@@ -313,6 +314,11 @@ class Context:
         h = _vp()
         _check(lib().sjcs_index_build_file(self._h, os.fsencode(str(path)), _c.byref(opts), _c.byref(h)))
         return Index(self, h, None)
+
+    def prepare_files(self, max_particles: int) -> None:
+        """Page-lock the file staging slots and grow the device pool for files
+        of up to max_particles (the first build_index_file then pays for neither)."""
+        _check(lib().sjcs_ctx_prepare_files(self._h, int(max_particles)))
 
     def build_index_compressed(self, uv, header: bytes, radius_hint: float = 0.0, kind: int = INDEX_GRID,
                                level: int = 0) -> "Index":

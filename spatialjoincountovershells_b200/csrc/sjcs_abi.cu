@@ -650,15 +650,22 @@ bool pread_all(int fd, char* dst, uint64_t off, uint64_t len) {
 // slot's previous copy before overwriting it.  idx's ev_start / ev_h2d
 // bracket the copies and the build stream waits for them.  Called with
 // ctx->ring_mu held.
+// The page-locked staging slots and their events (once per context; called
+// with ctx->ring_mu held).
+int ensure_ring(sjcs_ctx* ctx) {
+    if (ctx->ring) return SJCS_OK;
+    SJCS_CUDA_TRY(cudaMallocHost(&ctx->ring, (size_t)kIngestThreads * kIngestChunk));
+    ctx->ring_ev.assign(kIngestThreads, nullptr);
+    for (auto& e : ctx->ring_ev) SJCS_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    return SJCS_OK;
+}
+
 int ingest_file(sjcs_ctx* ctx, sjcs_index* idx, int fd, uint64_t bytes, void** d) {
     cudaStream_t u = ctx->s_h2d;
     const unsigned hw = std::max(1u, std::thread::hardware_concurrency());
     const unsigned T = std::min(kIngestThreads, hw);
-    if (!ctx->ring) {
-        SJCS_CUDA_TRY(cudaMallocHost(&ctx->ring, (size_t)kIngestThreads * kIngestChunk));
-        ctx->ring_ev.assign(kIngestThreads, nullptr);
-        for (auto& e : ctx->ring_ev) SJCS_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
-    }
+    int rc = ensure_ring(ctx);
+    if (rc) return rc;
     *d = nullptr;
     cudaEventRecord(idx->ev_start, u);
     cudaError_t e = cudaMallocAsync(d, bytes, u);
@@ -702,6 +709,22 @@ int ingest_file(sjcs_ctx* ctx, sjcs_index* idx, int fd, uint64_t bytes, void** d
     return SJCS_OK;
 }
 }  // namespace
+
+int sjcs_ctx_prepare_files(sjcs_ctx* ctx, uint64_t max_particles) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    {
+        std::lock_guard<std::mutex> lk(ctx->ring_mu);
+        rc = ensure_ring(ctx);
+        if (rc) return rc;
+    }
+    // one file's upload (12 B), sorted particles (16 B) and sort records and
+    // keys (44 B) per particle, the tile histograms, and the largest
+    // automatic cell table (2^27 + 1 entries)
+    const uint64_t bytes = max_particles * 73ull + (134217729ull * 4ull) + (64ull << 20);
+    return max_particles ? sjcs_ctx_reserve(ctx, bytes) : SJCS_OK;
+}
 
 int sjcs_index_build_file(sjcs_ctx* ctx, const char* path, const sjcs_index_opts* opts, sjcs_index** out) {
     if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");

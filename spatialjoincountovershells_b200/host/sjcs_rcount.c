@@ -29,6 +29,7 @@
  */
 #define _GNU_SOURCE
 #include <math.h>
+#include <pthread.h>
 #include <stdbool.h>
 #include <stdio.h>
 #include <stdlib.h>
@@ -144,6 +145,21 @@ static void die_lib(const char *what)
 /* ---- GPU options ------------------------------------------------------------ */
 
 static int g_index_kind = SJCS_INDEX_GRID;
+
+/* Context preparation for the particle files, run beside the halo parse. */
+static struct {
+    sjcs_ctx *ctx;
+    uint64_t n;
+    pthread_t th;
+    int started;
+} g_prepare;
+
+static void *prepare_files(void *arg)
+{
+    (void)arg;
+    sjcs_ctx_prepare_files(g_prepare.ctx, g_prepare.n);
+    return NULL;
+}
 static bool g_autotune = false;
 static bool g_compressed = false; /* --compressed: Gadget-encoded particle files, decoded on the GPU */
 
@@ -590,6 +606,18 @@ int main(int argc, char *argv[])
     /*** initialize ***/
     if (sjcs_ctx_create(0, &ctx) != SJCS_OK)
         die_lib("GPU context");
+    /* page-lock the file staging slots and grow the device pool for the
+     * largest particle file while the halo file is parsed */
+    {
+        uint64_t n, maxn = 0;
+        int k;
+        for (k = particle_beg; k < particle_end; ++k)
+            if (sjcs_particle_file_count(argv[k], &n) == 0 && n > maxn)
+                maxn = n;
+        g_prepare.ctx = ctx;
+        g_prepare.n = particle_compressed || use_graph ? 0 : maxn;
+        g_prepare.started = g_prepare.n && pthread_create(&g_prepare.th, NULL, prepare_files, &g_prepare) == 0;
+    }
 
     t0 = now_us();
     if (halo_filter_name == NULL) {
@@ -605,6 +633,8 @@ int main(int argc, char *argv[])
     }
     print_ms(">>>> halo data reading time", t0);
     printf("  # of halos = %lu\n", (unsigned long)nhalos);
+    if (g_prepare.started)
+        pthread_join(g_prepare.th, NULL); /* a failed preparation only means a slower first file */
 
     r2 = malloc(sizeof(float) * nrads);
     if (sjcs_radius_table(minrad, maxrad, nrads, r2) != SJCS_OK)

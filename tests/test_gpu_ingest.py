@@ -102,3 +102,18 @@ def test_concurrent_file_builds_from_several_threads(ctx, tmp_path):
         built[k].destroy()
         want, _ = _counts(ctx, lambda p=p: ctx.build_index(p, radius_hint=12), h, r2)
         assert np.array_equal(got, want), k
+
+
+def test_prepared_context_builds_the_same(tmp_path):
+    # a fresh context prepared for the files: same index as an unprepared one
+    rng = np.random.default_rng(21)
+    p = rng.uniform(0, 1000, size=(300_001, 3)).astype(np.float32)
+    h = rng.uniform(0, 1000, size=(800, 3)).astype(np.float32)
+    r2 = nat.radius_table(0.01, 15, 12)
+    path = tmp_path / "part.dat"
+    nat.write_particle_file(path, p)
+    with nat.Context(0) as c:
+        c.prepare_files(len(p))
+        c.prepare_files(0)  # nothing to do
+        got, _ = _counts(c, lambda: c.build_index_file(path, radius_hint=15), h, r2)
+    assert np.array_equal(got, oracle.count(p, h, r2))
