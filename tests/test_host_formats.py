@@ -2,6 +2,7 @@
 from __future__ import annotations
 
 import hashlib
+import pathlib
 
 import numpy as np
 import pytest
@@ -195,3 +196,25 @@ def test_halo_reader_floats_equal_strtof(tmp_path, built):
     assert np.array_equal(h["point"][:, 0].view(np.uint32), want.view(np.uint32))
     assert np.array_equal(h["point"][:, 1].view(np.uint32), want_y.view(np.uint32))
     assert np.array_equal(h["id"], np.arange(1, len(toks) + 1, dtype=np.uint64))
+
+
+def test_mapped_and_buffered_writers_agree(tmp_path, built):
+    # a regular file goes through the mapped writer, stdout through the
+    # buffered one; both must give the same text
+    import subprocess
+    import sys
+    rng = np.random.default_rng(3)
+    halos = nat.gen_uniform_halos(4, 3000)
+    counts = rng.integers(0, 10 ** 9, size=(3000, 24)).astype(np.uint64)
+    r2 = nat.radius_table(0.01, 7.0, 24)
+    np.save(tmp_path / "c.npy", counts)
+    np.save(tmp_path / "h.npy", halos)
+    nat.write_result(tmp_path / "mapped.txt", halos, r2, counts, nthreads=5)
+    code = ("import sys, numpy as np; sys.path.insert(0, sys.argv[1]); "
+            "from spatialjoincountovershells_b200 import _native as nat; "
+            "nat.write_result(None, np.load(sys.argv[2]), nat.radius_table(0.01, 7.0, 24), np.load(sys.argv[3]), "
+            "nthreads=5)")
+    root = str(pathlib.Path(__file__).resolve().parents[1])
+    out = subprocess.run([sys.executable, "-c", code, root, str(tmp_path / "h.npy"), str(tmp_path / "c.npy")],
+                         capture_output=True, check=True).stdout
+    assert out == (tmp_path / "mapped.txt").read_bytes()
