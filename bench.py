@@ -191,32 +191,49 @@ def ref_threads() -> int:
     return max(1, min(n - 1, 64))
 
 
-def reference_sample(w, particles_file0, tmp: pathlib.Path, nhalos_sample: int):
-    """Write the reference's inputs for one file and a halo prefix sample."""
+def write_reference_inputs(tmp: pathlib.Path, particles, nfiles: int, halos):
+    """Particle files and a halo file in the reference's formats (our arm:
+    written by this package's host library from the arrays it counts)."""
     from spatialjoincountovershells_b200 import _native as nat
-    pf = tmp / "part0.dat"
-    if not pf.exists():
-        nat.write_particle_file(pf, particles_file0)
+    n = len(particles) // nfiles
+    files = []
+    for f in range(nfiles):
+        pf = tmp / f"part{f}.dat"
+        nat.write_particle_file(pf, particles[f * n:(f + 1) * n])
+        files.append(pf)
     hf = tmp / "halo_sample.list"
-    if not hf.exists():
-        nat.gen_uniform_halo_file(hf, w["hseed"], nhalos_sample)
-    return pf, hf
+    nat.write_halo_file(hf, halos)
+    return files, hf
 
 
-def run_reference_once(w, pf, hf, threads: int):
+def run_reference(files, hf, radius, threads: int, result: bool, timeout=1800):
+    """astr_rcount over the particle files and the halo file (same directory).
+    Returns its phase times (seconds per file: build, search), wall time and,
+    with result=True, its counts parsed from the result text."""
     from oracle import oracle
-    mn, mx, nr = w["radius"]
-    r = oracle.run_ref(["--thread", threads, "--next-setup", threads, "--particle-files", pf.name,
-                        "--halo-file", hf.name, "--radius", f"{mn}:{mx}:{nr}", "--output-file", "/dev/null"],
-                       cwd=pf.parent, timeout=1800)
+    mn, mx, nr = radius
+    tmp = files[0].parent
+    out = tmp / "ref_result.txt"
+    t0 = time.perf_counter()
+    r = oracle.run_ref(["--thread", threads, "--next-setup", threads, "--particle-files", *[f.name for f in files],
+                        "--halo-file", hf.name, "--radius", f"{mn}:{mx}:{nr}",
+                        "--output-file", out.name if result else "/dev/null"], cwd=tmp, timeout=timeout)
+    wall = time.perf_counter() - t0
     if r.returncode != 0:
         raise RuntimeError(f"reference failed: {r.stderr[-500:]}")
     t = oracle.ref_phase_times(r.stdout)
-    return t.get("index construction", 0) / 1e3, t.get("searching", 0) / 1e3
+    res = {"build_s": t.get("index construction", 0) / 1e3 / len(files),
+           "search_s": t.get("searching", 0) / 1e3 / len(files), "wall_s": wall, "counts": None}
+    if result:
+        _, counts, _ = oracle.parse_result_text(out.read_bytes(), nr)
+        res["counts"] = counts
+        out.unlink()
+    return res
 
 
 def reference_extrapolate(w, build_s: float, search_s: float, nhalos_sample: int) -> float:
-    """Halo-file passes per second of the full workload from one sampled file."""
+    """Halo-file passes per second of the full workload from sampled files
+    (build and search seconds per file; search scaled by the halo count)."""
     full_s = w["nfiles"] * (build_s + search_s * w["nhalos"] / nhalos_sample)
     return w["nhalos"] * w["nfiles"] / full_s
 
@@ -228,6 +245,18 @@ def port_baseline(w, particles_file0, halos_sample, r2):
     oracle.count(particles_file0, halos_sample, r2, nthreads=1)
     dt = time.perf_counter() - t0
     return w["nhalos"] * w["nfiles"] / (w["nfiles"] * dt * w["nhalos"] / len(halos_sample))
+
+
+def parity_record(ref_counts, forms: dict, workload: str, radius) -> dict:
+    """Per index form: are its counts for the sampled halos identical to the reference's?"""
+    import numpy as np
+    m = len(ref_counts)
+    res = {name: bool(np.array_equal(c[:m].astype(np.uint64), ref_counts)) for name, c in forms.items()}
+    mn, mx, nr = radius
+    return {"identical": all(res.values()), "halo_rows_compared": int(m), "shells": int(nr),
+            "counts_compared": int(m * nr * len(forms)), "forms": res,
+            "reference_total": int(ref_counts.sum()), "workload": workload,
+            "against": "astr_rcount result text (the reference compiled from its sources), all particle files"}
 
 
 # ---------------------------------------------------------------------------
@@ -391,6 +420,7 @@ def run_ours(args, w, dist, rank, world, local):
         ms_e2e = dist_max(dist, ms_e2e, local)
 
     # one extra untimed pass for the per-phase split (build vs search)
+    nhs = min(nh, 100_000)  # halos compared with the reference program (a prefix of the halo stream)
     q = ctx.query(halos_d, r2)
     bt = []
     for f in range(nf):
@@ -401,8 +431,27 @@ def run_ours(args, w, dist, rank, world, local):
         idx.destroy()
     qt = q.timing()
     q.wait()
-    grid_counts = device_counts(q) if not args.no_forms else None
+    grid_counts = device_counts(q)
+    sample = {"grid": grid_counts[:nhs * nr].cpu().numpy().view(np.uint32).reshape(nhs, nr)}
     q.destroy()
+
+    def counts_of(kind, mode):
+        qq = ctx.query(halos_d, r2)
+        qq.set_schedule(mode)
+        for f in range(nf):
+            ix = ctx.build_index(parts_d[f], radius_hint=R, kind=kind)
+            qq.count(ix)
+            ix.destroy()
+        qq.wait()
+        c = device_counts(qq)
+        qq.destroy()
+        return c
+
+    # the persistent-queue schedule on the same index: same counts on the device
+    c = counts_of(nat.INDEX_GRID, nat.SCHED_QUEUE)
+    queue_same = bool(torch.equal(c, grid_counts))
+    sample["grid-queue"] = c[:nhs * nr].cpu().numpy().view(np.uint32).reshape(nhs, nr)
+    del c
 
     # the other index forms on the same workload (resident leg): the learned
     # index and the plain Morton table, with their counts compared on the device
@@ -429,7 +478,10 @@ def run_ours(args, w, dist, rank, world, local):
                     info = ix.learned_info()
                 ix.destroy()
             qq.wait()
-            same = bool(torch.equal(device_counts(qq), grid_counts))
+            c = device_counts(qq)
+            same = bool(torch.equal(c, grid_counts))
+            sample[name] = c[:nhs * nr].cpu().numpy().view(np.uint32).reshape(nhs, nr)
+            del c
             qq.destroy()
             forms[name] = {"value": round(nh * nf * world / (fms / 1e3), 1), "ms_per_step": round(fms, 3),
                            "build_s_per_file": round(statistics.mean(fb) / 1e3, 5),
@@ -438,7 +490,8 @@ def run_ours(args, w, dist, rank, world, local):
             if info:
                 forms[name]["model"] = {"leaves": info["leaves"], "max_err": info["max_err"],
                                         "mean_err": round(info["mean_err"], 1), "level": info["level"]}
-        del grid_counts
+    del grid_counts
+    torch.cuda.empty_cache()
 
     units = nh * nf * world
     value = units / (ms / 1e3)
@@ -453,9 +506,15 @@ def run_ours(args, w, dist, rank, world, local):
                 "algorithmic_bytes_per_launch": ALGO_BYTES_PER_HALO_FILE * nh,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
 
-    cpu = None
+    # the reference program on the same host: every particle file of the
+    # step and the first nhs halos; its result text is the parity check of
+    # every form above at the timed configuration
+    cpu, parity = None, None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_baseline_leg(w, pnp[:n], halos_np, r2)
+        cpu, ref_counts = reference_leg(w, pnp, halos_np[:nhs], r2)
+        if ref_counts is not None:
+            parity = parity_record(ref_counts, sample, workload_name(w), w["radius"])
+    del sample
 
     line = {
         "metric": METRIC, "value": round(value, 1), "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
@@ -480,7 +539,9 @@ def run_ours(args, w, dist, rank, world, local):
         "clocks_e2e": clocks_e2e,
         "gpu_launches": int(launches),
         "gpu_launches_e2e": int(launches_e2e),
+        "queue_schedule_counts_identical_to_static": queue_same,
         "forms": forms,
+        "parity_at_scale": {"c2": parity} if parity else None,
     }
     ctx.close()
     return line
@@ -581,50 +642,87 @@ def time_steps(ctx, step, K, W, dist, local):
     return ms, int(launches), (cnt / calls if calls else None), clk.summary()
 
 
-def reference_sample_clustered(w, particles_file0, halos_sample, tmp: pathlib.Path):
-    from spatialjoincountovershells_b200 import _native as nat
-    pf, hf = tmp / "part0.dat", tmp / "halo_sample.list"
-    nat.write_particle_file(pf, particles_file0)
-    nat.write_halo_file(hf, halos_sample)
-    return pf, hf
+class ClusteredData:
+    """Inputs of the clustered workloads (C3, C4, C5): pinned host copies of
+    every file and of the halos, and resident device copies."""
+
+    def __init__(self, w, local):
+        import torch
+
+        from spatialjoincountovershells_b200 import _native as nat
+        n, nf = w["nparticles"], w["nfiles"]
+        self.w = w
+        self.parts_h = torch.empty((nf * n, 3), dtype=torch.float32, pin_memory=True)
+        self.pnp = self.parts_h.numpy()
+        for f in range(nf):
+            self.pnp[f * n:(f + 1) * n] = nat.gen_clustered_particles(w["pseed"] + f, n)
+        halos = nat.gen_clustered_halos(w["hseed"], w["nhalos"])
+        self.halos_h = torch.empty((w["nhalos"] * 24,), dtype=torch.uint8, pin_memory=True)
+        self.hnp = self.halos_h.numpy().view(nat.HALO_DTYPE)
+        self.hnp[:] = halos
+        import numpy as np
+        self.parts_d = [torch.from_numpy(self.pnp[f * n:(f + 1) * n]).to(f"cuda:{local}") for f in range(nf)]
+        self.halos_d = torch.from_numpy(np.ascontiguousarray(halos["point"])).to(f"cuda:{local}")
+        torch.cuda.synchronize()
+
+    def release_device(self):
+        import torch
+        self.parts_d = None
+        self.halos_d = None
+        torch.cuda.empty_cache()
 
 
-def clustered_cpu_baseline(w, particles_file0, halos, nhs):
+def clustered_reference_legs(w, data, legs):
+    """astr_rcount on every clustered particle file (written once) for each
+    (name, radius, nhalos_sample) leg.  Returns {name: run_reference result}."""
     from oracle import oracle
     if not oracle.ref_available():
-        return None
+        return {}
+    from spatialjoincountovershells_b200 import _native as nat
+    T = ref_threads()
+    out = {}
     with tempfile.TemporaryDirectory(prefix="sjcs_refcl_") as td:
-        pf, hf = reference_sample_clustered(w, particles_file0, halos[:nhs], pathlib.Path(td))
-        T = ref_threads()
-        b, s_ = run_reference_once(w, pf, hf, T)
-    v = w["nhalos"] * w["nfiles"] / (w["nfiles"] * (b + s_ * w["nhalos"] / nhs))
-    return {"value": round(v, 1), "unit": UNIT, "cores": T, "kind": "reference",
-            "sample": f"astr_rcount --thread {T} --next-setup {T} on 1 clustered file of {w['nparticles']:.0e} "
-                      f"particles x the first {nhs} halos; build {b:.3f} s, search {s_:.3f} s; extrapolated to "
-                      f"{w['nfiles']} files x {w['nhalos']:.0e} halos"}
+        tmp = pathlib.Path(td)
+        n, nf = w["nparticles"], w["nfiles"]
+        files = []
+        for f in range(nf):
+            pf = tmp / f"part{f}.dat"
+            nat.write_particle_file(pf, data.pnp[f * n:(f + 1) * n])
+            files.append(pf)
+        for name, radius, nhs in legs:
+            hf = tmp / f"halos_{name}.list"
+            nat.write_halo_file(hf, data.hnp[:nhs])
+            r = run_reference(files, hf, radius, T, result=True)
+            r["threads"] = T
+            r["nhs"] = nhs
+            out[name] = r
+            hf.unlink()
+    return out
 
 
-def run_clustered(args, w, dist, rank, world, local):
-    """C3: clustered uneven load; autotuned persistent schedule; captured file steps."""
+def clustered_cpu_baseline(w, r) -> dict:
+    b, s = r["build_s"], r["search_s"]
+    return {"value": round(reference_extrapolate(w, b, s, r["nhs"]), 1), "unit": UNIT, "cores": r["threads"],
+            "kind": "reference",
+            "sample": f"astr_rcount --thread {r['threads']} --next-setup {r['threads']} on all {w['nfiles']} "
+                      f"clustered files of {w['nparticles']:.0e} particles x the first {r['nhs']} halos: build "
+                      f"{b:.3f} s and search {s:.3f} s per file (wall {r['wall_s']:.1f} s); extrapolated to "
+                      f"{w['nhalos']:.0e} halos"}
+
+
+def section_c3(args, w, ctx, data, K, W, dist, local, world, nhs):
+    """C3: clustered uneven load; autotuned persistent schedule vs static;
+    captured file steps; e2e.  Returns (section, counts of the first nhs halos
+    per schedule)."""
     import numpy as np
-    import torch
 
     from spatialjoincountovershells_b200 import _native as nat
-    torch.cuda.set_device(local)
     n, nf, nh = w["nparticles"], w["nfiles"], w["nhalos"]
     mn, mx, nr = w["radius"]
     r2 = nat.radius_table(mn, mx, nr)
     R = math.sqrt(float(r2[-1]))
-    parts_h, halos_h, hnp, hpts = clustered_inputs(w)
-    pnp = parts_h.numpy()
+    pnp, hnp, parts_d, halos_d = data.pnp, data.hnp, data.parts_d, data.halos_d
     out_np = np.empty((nh, nr), np.uint64)
-    ctx = nat.Context(local)
-    ctx.set_overlap(args.overlap)
-    if not args.no_reserve:
-        ctx.reserve(4 * (n * 16 + int(1.6 * n + 4096) * 4) + n * 44 + 4 * nh * (16 + 4 * nr + 64) + (2 << 30))
-    parts_d = [torch.from_numpy(pnp[f * n:(f + 1) * n]).cuda() for f in range(nf)]
-    halos_d = torch.from_numpy(hpts).cuda()
-    torch.cuda.synchronize()
 
     # autotune on file 0 (the choice is cached in the context for this shape)
     idx0 = ctx.build_index(parts_d[0], radius_hint=R)
@@ -653,10 +751,18 @@ def run_clustered(args, w, dist, rank, world, local):
         q.read_counts(out=out_np)
         return q
 
-    K, W = args.steps, args.warmup
     ms, launches, count_ms, clocks = time_steps(ctx, step_resident(nat.SCHED_AUTO), K, W, dist, local)
     ms_static, _, count_static, _ = time_steps(ctx, step_resident(nat.SCHED_STATIC), K, W, dist, local)
     ms_e2e, launches_e2e, _, clocks_e2e = time_steps(ctx, step_e2e, K, W, dist, local)
+
+    sample = {}
+    for name, mode in (("grid-queue", nat.SCHED_QUEUE), ("grid-static", nat.SCHED_STATIC)):
+        q = step_resident(mode)()
+        q.wait()
+        c = device_counts(q)
+        sample[name] = c[:nhs * nr].cpu().numpy().view(np.uint32).reshape(nhs, nr)
+        q.destroy()
+        del c
 
     # captured file steps (graph replays of copy + build + count) against the
     # same query, after W warm-up replays
@@ -671,15 +777,12 @@ def run_clustered(args, w, dist, rank, world, local):
     st.destroy()
     q.destroy()
 
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        cpu = clustered_cpu_baseline(w, pnp[:n], hnp, 2000)
     units = nh * nf * world
-    line = {
+    sec = {
         "metric": "halos/s (clustered uneven load, persistent schedule)", "value": round(units / (ms / 1e3), 1),
         "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W, "ms_per_step": round(ms, 3),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: project generators (clumped particles and halos, MT19937)",
+        "data": "synthetic: project generators (clumped particles and halos, MT19937 block streams)",
         "config": {"workload": clustered_name(w), "index": "grid", "schedule": tune["chosen"],
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": f"inputs larger than L2 ({nf} x {n * 12 / 1e9:.2f} GB particle arrays per step)"},
@@ -690,32 +793,25 @@ def run_clustered(args, w, dist, rank, world, local):
         "captured_step_ms_per_file": round(statistics.mean(gms), 3),
         "e2e": {"value": round(units / (ms_e2e / 1e3), 1), "unit": UNIT, "ms_per_step": round(ms_e2e, 3),
                 "h2d_bytes_per_step": int(nf * n * 12 + (nh - 1) * 24 + 12), "d2h_bytes_per_step": int(nh * nr * 8)},
-        "roofline": None, "cpu_baseline": cpu, "clocks": clocks, "clocks_e2e": clocks_e2e,
+        "roofline": None, "clocks": clocks, "clocks_e2e": clocks_e2e,
         "gpu_launches": launches, "gpu_launches_e2e": launches_e2e,
     }
-    ctx.close()
-    return line
+    return sec, sample
 
 
-def run_forms(args, w, dist, rank, world, local):
-    """C4: learned index vs plain forms on the clustered data, counts compared on the device."""
+def section_c4(args, w, ctx, data, K, W, dist, local, world, nhs):
+    """C4: learned index vs plain forms on the clustered data, each form's
+    counts compared on the device with the first form's.  Returns (section,
+    counts of the first nhs halos per form)."""
+    import numpy as np
     import torch
 
     from spatialjoincountovershells_b200 import _native as nat
-    torch.cuda.set_device(local)
     n, nf, nh = w["nparticles"], w["nfiles"], w["nhalos"]
     mn, mx, nr = w["radius"]
     r2 = nat.radius_table(mn, mx, nr)
     R = math.sqrt(float(r2[-1]))
-    parts_h, halos_h, hnp, hpts = clustered_inputs(w)
-    pnp = parts_h.numpy()
-    ctx = nat.Context(local)
-    ctx.set_overlap(args.overlap)
-    if not args.no_reserve:
-        ctx.reserve(4 * (n * 16 + int(1.6 * n + 4096) * 4) + n * 60 + 4 * nh * (16 + 4 * nr + 64) + (2 << 30))
-    parts_d = [torch.from_numpy(pnp[f * n:(f + 1) * n]).cuda() for f in range(nf)]
-    halos_d = torch.from_numpy(hpts).cuda()
-    torch.cuda.synchronize()
+    parts_d, halos_d = data.parts_d, data.halos_d
     # every form gets its own autotuned schedule (cached in the context per index kind)
     tunes = {}
     for kind in (nat.INDEX_GRID, nat.INDEX_MORTON, nat.INDEX_LEARNED):
@@ -724,13 +820,11 @@ def run_forms(args, w, dist, rank, world, local):
         tunes[kind] = ctx.autotune(qt, idx0)
         qt.destroy()
         idx0.destroy()
-    tune = tunes[nat.INDEX_GRID]
 
     forms = [("grid", nat.INDEX_GRID, nat.SCHED_AUTO), ("grid-static", nat.INDEX_GRID, nat.SCHED_STATIC),
              ("morton", nat.INDEX_MORTON, nat.SCHED_AUTO), ("morton-static", nat.INDEX_MORTON, nat.SCHED_STATIC),
              ("learned", nat.INDEX_LEARNED, nat.SCHED_AUTO), ("learned-static", nat.INDEX_LEARNED, nat.SCHED_STATIC)]
-    K, W = args.steps, args.warmup
-    res, ref_counts, info = {}, None, None
+    res, first, info, sample = {}, None, None, {}
     for name, kind, mode in forms:
         def step(kind=kind, mode=mode):
             q = ctx.query(halos_d, r2)
@@ -755,31 +849,126 @@ def run_forms(args, w, dist, rank, world, local):
             idx.destroy()
         q.wait()
         c = device_counts(q)
-        if ref_counts is None:
-            ref_counts = c
+        sample[name] = c[:nhs * nr].cpu().numpy().view(np.uint32).reshape(nhs, nr)
+        if first is None:
+            first = c
             same = True
         else:
-            same = bool(torch.equal(c, ref_counts))
+            same = bool(torch.equal(c, first))
+        del c
         q.destroy()
         res[name] = {"value": round(nh * nf * world / (ms / 1e3), 1), "ms_per_step": round(ms, 3),
                      "build_s_per_file": round(statistics.mean(bts) / 1e3, 5),
                      "count_ms_per_file": round(count_ms, 3) if count_ms else None,
                      "counts_identical_to_grid": same, "gpu_launches": launches, "clocks": clocks,
                      "schedule": tunes[kind]["chosen"] if mode == nat.SCHED_AUTO else "static"}
-    del ref_counts
-    line = {
+    del first
+    torch.cuda.empty_cache()
+    sec = {
         "metric": METRIC, "value": res["learned"]["value"], "unit": UNIT, "n_gpus": world, "steps": K,
         "warmup": W, "ms_per_step": res["learned"]["ms_per_step"], "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32",
-        "data": "synthetic: project generators (clumped particles and halos, MT19937)",
+        "data": "synthetic: project generators (clumped particles and halos, MT19937 block streams)",
         "config": {"workload": clustered_name(w), "index": "learned (63-bit Morton, 2-level PLM, 4096 leaves)",
-                   "parallelism": "replicas" if world > 1 else "single", "grid_schedule": tune["chosen"]},
-        "plain_value": res["grid"]["value"], "forms": res,
+                   "parallelism": "replicas" if world > 1 else "single",
+                   "grid_schedule": tunes[nat.INDEX_GRID]["chosen"]},
+        "plain_value": res["grid"]["value"],
+        "learned_over_plain": round(res["learned"]["value"] / res["grid"]["value"], 3),
+        "forms": res,
         "learned_info": {k: (round(v, 3) if isinstance(v, float) else v) for k, v in (info or {}).items()},
         "gpu_launches": res["learned"]["gpu_launches"], "clocks": res["learned"]["clocks"],
     }
+    return sec, sample
+
+
+C3_SAMPLE, C4_SAMPLE = 2000, 100_000  # halos of the clustered workloads compared with the reference
+
+
+def clustered_context(args, w, local, extra_per_particle):
+    from spatialjoincountovershells_b200 import _native as nat
+    n, nh = w["nparticles"], w["nhalos"]
+    nr = w["radius"][2]
+    ctx = nat.Context(local)
+    ctx.set_overlap(args.overlap)
+    if not args.no_reserve:
+        ctx.reserve(4 * (n * 16 + int(1.6 * n + 4096) * 4) + n * extra_per_particle + 4 * nh * (16 + 4 * nr + 64)
+                    + (2 << 30))
+    return ctx
+
+
+def run_clustered(args, w, dist, rank, world, local):
+    """C3 on its own line (--workload clustered)."""
+    import torch
+    torch.cuda.set_device(local)
+    data = ClusteredData(w, local)
+    ctx = clustered_context(args, w, local, 44)
+    sec, sample = section_c3(args, w, ctx, data, args.steps, args.warmup, dist, local, world, C3_SAMPLE)
     ctx.close()
-    return line
+    data.release_device()
+    sec["cpu_baseline"] = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        refs = clustered_reference_legs(w, data, [("c3", w["radius"], C3_SAMPLE)])
+        if "c3" in refs:
+            sec["cpu_baseline"] = clustered_cpu_baseline(w, refs["c3"])
+            sec["parity_at_scale"] = {"c3_sample": parity_record(refs["c3"]["counts"], sample, clustered_name(w),
+                                                                 w["radius"])}
+    return sec
+
+
+def run_forms(args, w, dist, rank, world, local):
+    """C4 on its own line (--workload learned)."""
+    import torch
+    torch.cuda.set_device(local)
+    data = ClusteredData(w, local)
+    ctx = clustered_context(args, w, local, 60)
+    sec, sample = section_c4(args, w, ctx, data, args.steps, args.warmup, dist, local, world, C4_SAMPLE)
+    ctx.close()
+    data.release_device()
+    sec["cpu_baseline"] = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        refs = clustered_reference_legs(w, data, [("c4", w["radius"], C4_SAMPLE)])
+        if "c4" in refs:
+            sec["cpu_baseline"] = clustered_cpu_baseline(w, refs["c4"])
+            sec["parity_at_scale"] = {"c4_sample": parity_record(refs["c4"]["counts"], sample, clustered_name(w),
+                                                                 w["radius"])}
+    return sec
+
+
+def run_extras(args, dist, rank, world, local, K, W, small):
+    """Configs 3-5 for the headline line: C3 and C4 on one clustered data set
+    (reference parity samples for both), then C5 over resident indexes of the
+    same particles.  K timed and W warm-up steps per leg."""
+    import torch
+    c3, c4 = dict(CLUSTERED), dict(FORMS)
+    sv = dict(SERVING, nrequests=SERVING_IN_HEADLINE)
+    if small:
+        for d in (c3, c4, sv):
+            d["nparticles"] //= 50
+            if "nhalos" in d:
+                d["nhalos"] //= 50
+        sv["nrequests"] //= 10
+        sv["size"] = (sv["size"][0], sv["size"][1] / 50)
+    data = ClusteredData(c3, local)
+    out = {}
+    ctx = clustered_context(args, c3, local, 60)
+    out["clustered_c3"], s3 = section_c3(args, c3, ctx, data, K, W, dist, local, world, min(C3_SAMPLE, c3["nhalos"]))
+    out["forms_clustered_c4"], s4 = section_c4(args, c4, ctx, data, K, W, dist, local, world,
+                                               min(C4_SAMPLE, c4["nhalos"]))
+    ctx.close()
+    torch.cuda.empty_cache()
+    parity = {}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        refs = clustered_reference_legs(c3, data, [("c3", c3["radius"], min(C3_SAMPLE, c3["nhalos"])),
+                                                   ("c4", c4["radius"], min(C4_SAMPLE, c4["nhalos"]))])
+        if refs:
+            out["clustered_c3"]["cpu_baseline"] = clustered_cpu_baseline(c3, refs["c3"])
+            out["forms_clustered_c4"]["cpu_baseline"] = clustered_cpu_baseline(c4, refs["c4"])
+            parity["c3_sample"] = parity_record(refs["c3"]["counts"], s3, clustered_name(c3), c3["radius"])
+            parity["c4_sample"] = parity_record(refs["c4"]["counts"], s4, clustered_name(c4), c4["radius"])
+    out["serving_c5"] = run_serving(args, sv, dist, rank, world, local, data=data)
+    data.release_device()
+    del data
+    return out, parity
 
 
 def run_io(args, w, dist, rank, world, local):
@@ -843,8 +1032,12 @@ def run_io(args, w, dist, rank, world, local):
     }
 
 
-def run_serving(args, w, dist, rank, world, local):
-    """C5: request loop over resident clustered indexes, Poisson arrivals, p50/p99."""
+SERVING_IN_HEADLINE = 400  # requests of the serving leg inside the headline line (a prefix of the stream)
+
+
+def run_serving(args, w, dist, rank, world, local, data=None):
+    """C5: request loop over resident clustered indexes, Poisson arrivals, p50/p99.
+    data: resident clustered particles to index (else generated here)."""
     import numpy as np
     import torch
 
@@ -863,10 +1056,15 @@ def run_serving(args, w, dist, rank, world, local):
     ctx = nat.Context(local)
     idx = []
     for f in range(nf):
-        p = torch.from_numpy(nat.gen_clustered_particles(w["pseed"] + f, n)).cuda()
+        if data is not None:
+            p = data.parts_d[f]
+        else:
+            p = torch.from_numpy(nat.gen_clustered_particles(w["pseed"] + f, n)).cuda()
         idx.append(ctx.build_index(p, radius_hint=w["rmax"][1]))
         idx[-1].wait()
         del p
+    if data is not None:
+        data.release_device()
     torch.cuda.empty_cache()
     ctx.trim()
 
@@ -962,23 +1160,26 @@ def run_serving(args, w, dist, rank, world, local):
     }
 
 
-def cpu_baseline_leg(w, particles_file0, halos, r2):
+def reference_leg(w, particles, halos_sample, r2):
+    """cpu_baseline and parity check: astr_rcount (compiled from the reference's
+    sources) over every particle file of the workload and a halo sample, on
+    this host's cores.  Returns (cpu_baseline, counts of the sampled halos)."""
     from oracle import oracle
-    nhs = 100_000 if w["nhalos"] >= 1_000_000 else max(1000, w["nhalos"] // 10)
+    nhs = len(halos_sample)
+    if not oracle.ref_available():
+        v = port_baseline(w, particles[:w["nparticles"]], halos_sample[:1000], r2)
+        return ({"value": round(v, 1), "unit": UNIT, "cores": 1, "kind": "port",
+                 "sample": "oracle port, 1 thread, 1 file x 1000 halos, extrapolated"}, None)
+    T = ref_threads()
     with tempfile.TemporaryDirectory(prefix="sjcs_ref_") as td:
-        tmp = pathlib.Path(td)
-        if oracle.ref_available():
-            pf, hf = reference_sample(w, particles_file0, tmp, nhs)
-            T = ref_threads()
-            b, s = run_reference_once(w, pf, hf, T)
-            return {"value": round(reference_extrapolate(w, b, s, nhs), 1), "unit": UNIT, "cores": T,
-                    "kind": "reference",
-                    "sample": f"astr_rcount --thread {T} --next-setup {T} on 1 file of {w['nparticles']:.0e} "
-                              f"particles x {nhs} halos (prefix of the halo stream); build {b:.3f} s, search "
-                              f"{s:.3f} s; extrapolated to {w['nfiles']} files x {w['nhalos']:.0e} halos"}
-        v = port_baseline(w, particles_file0, halos[:nhs], r2)
-        return {"value": round(v, 1), "unit": UNIT, "cores": 1, "kind": "port",
-                "sample": f"oracle port, 1 thread, 1 file x {nhs} halos, extrapolated"}
+        files, hf = write_reference_inputs(pathlib.Path(td), particles, w["nfiles"], halos_sample)
+        r = run_reference(files, hf, w["radius"], T, result=True)
+    b, s = r["build_s"], r["search_s"]
+    cpu = {"value": round(reference_extrapolate(w, b, s, nhs), 1), "unit": UNIT, "cores": T, "kind": "reference",
+           "sample": f"astr_rcount --thread {T} --next-setup {T} on all {w['nfiles']} files of "
+                     f"{w['nparticles']:.0e} particles x the first {nhs} halos: build {b:.3f} s and search "
+                     f"{s:.3f} s per file (wall {r['wall_s']:.1f} s); extrapolated to {w['nhalos']:.0e} halos"}
+    return cpu, r["counts"]
 
 
 # ---------------------------------------------------------------------------
@@ -986,41 +1187,69 @@ def cpu_baseline_leg(w, particles_file0, halos, r2):
 # ---------------------------------------------------------------------------
 
 def run_reference_arm(args, w):
+    """The reference program alone, as stock as it ships: its own generators
+    write the inputs (MT19937 seeds as our arm's), astr_rcount counts them.
+    No library of this package is loaded in this process.  One step is a
+    bounded sample of the workload: one whole particle file (built, as
+    every file is) and the first nhs halos searched against it; files rotate
+    over the workload's files.  ms_per_step is that measured sample; value
+    is the whole workload's halo-file passes per second extrapolated from
+    the mean sample (build time per file, search time scaled by the halo
+    count), under "extrapolation"."""
     from oracle import oracle
-
-    from spatialjoincountovershells_b200 import _native as nat
     if not oracle.ref_available():
         return {"impl": "reference", "metric": METRIC, "unit": UNIT,
                 "unavailable": "reference program not built (oracle/_ref/astr_rcount.exe missing)"}
     nhs = 100_000 if w["nhalos"] >= 1_000_000 else max(1000, w["nhalos"] // 10)
+    nf, n = w["nfiles"], w["nparticles"]
     T = ref_threads()
+
+    def gen(exe, paths, count, seed):
+        r = subprocess.run([str(exe), "-f", *[str(x) for x in paths], "-n", str(count), "-s", str(seed)],
+                           capture_output=True, text=True, timeout=1800)
+        if r.returncode != 0:
+            raise RuntimeError(f"{exe.name} failed: {r.stderr[-300:]}")
+
     with tempfile.TemporaryDirectory(prefix="sjcs_refarm_") as td:
         tmp = pathlib.Path(td)
-        p0 = nat.gen_uniform_particles(w["pseed"], 1, w["nparticles"])
-        pf, hf = reference_sample(w, p0, tmp, nhs)
-        del p0
+        t0 = time.perf_counter()
+        files = [tmp / f"part{f}.dat" for f in range(nf)]
+        gen(oracle.REF_PGEN, files, n, w["pseed"])   # one stream over the files, as main.c:42-68
+        hf = tmp / "halos.list"
+        gen(oracle.REF_HGEN, [hf], nhs, w["hseed"])  # the halo stream's first nhs halos
+        gen_s = time.perf_counter() - t0
         # warm-up runs on a small file (untimed): page in the binary and the inputs' cache
-        small = tmp / "warm"
-        small.mkdir()
-        wpf, whf = reference_sample(dict(w, nparticles=1_000_000), nat.gen_uniform_particles(w["pseed"], 1, 1_000_000),
-                                    small, min(nhs, 10_000))
+        warm = tmp / "warm"
+        warm.mkdir()
+        wpf, whf = warm / "part.dat", warm / "halos.list"
+        gen(oracle.REF_PGEN, [wpf], 1_000_000, w["pseed"])
+        gen(oracle.REF_HGEN, [whf], 10_000, w["hseed"])
         for _ in range(args.warmup):
-            run_reference_once(w, wpf, whf, T)
-        times = [run_reference_once(w, pf, hf, T) for _ in range(args.steps)]
-    b = statistics.mean(t[0] for t in times)
-    s = statistics.mean(t[1] for t in times)
+            run_reference([wpf], whf, w["radius"], T, result=False)
+        runs = []
+        for k in range(args.steps):
+            runs.append(run_reference([files[k % nf]], hf, w["radius"], T, result=False))
+    b = statistics.mean(r["build_s"] for r in runs)
+    s = statistics.mean(r["search_s"] for r in runs)
+    step_ms = 1e3 * (b + s)
     v = reference_extrapolate(w, b, s, nhs)
-    full_ms = 1e3 * w["nhalos"] * w["nfiles"] / v
-    sample = (f"astr_rcount --thread {T} --next-setup {T}: per step 1 file of {w['nparticles']:.0e} particles "
-              f"(build {b:.3f} s) and {nhs} halos (search {s:.3f} s), extrapolated to {w['nfiles']} files x "
-              f"{w['nhalos']:.0e} halos")
+    full_ms = 1e3 * w["nhalos"] * nf / v
+    sample = (f"astr_rcount --thread {T} --next-setup {T}: per step 1 file of {n:.0e} particles (build {b:.3f} s) "
+              f"and the first {nhs} halos (search {s:.3f} s); files rotate over the {nf} files")
     return {
         "impl": "reference", "metric": METRIC, "value": round(v, 1), "unit": UNIT, "n_gpus": 0,
-        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(full_ms, 1), "higher_is_better": True,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(step_ms, 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": round(v / PUBLISHED_HALO_FILES_PER_S, 3), "dtype": "f32",
-        "data": "synthetic: reference generator streams (MT19937 seeds 1 and 2)",
-        "config": {"workload": workload_name(w), "index": "reference STR tree (CPU)", "parallelism": "cpu threads"},
+        "data": "synthetic: the reference's own generators (uniform_decoded_particle_generator -s "
+                f"{w['pseed']}, uniform_halo_generator -s {w['hseed']})",
+        "config": {"workload": workload_name(w), "index": "reference STR tree (CPU)", "parallelism": "cpu threads",
+                   "step": f"1 particle file x {nhs} halos (bounded sample of the workload)"},
         "build_s_per_file": round(b, 3),
+        "wall_ms_per_step": round(1e3 * statistics.mean(r["wall_s"] for r in runs), 1),
+        "extrapolation": {"full_step_ms": round(full_ms, 1),
+                          "method": f"{nf} x (build per file + search per file x {w['nhalos']} / {nhs})",
+                          "value": round(v, 1)},
+        "input_generation_s": round(gen_s, 1),
         "cpu_baseline": {"value": round(v, 1), "unit": UNIT, "cores": T, "kind": "reference", "sample": sample},
         "e2e": {"value": round(v, 1), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -1042,6 +1271,10 @@ def main():
     ap.add_argument("--no-check", action="store_true",
                     help="accepted and ignored (parity is checked by the test suite, not by the benchmark)")
     ap.add_argument("--no-forms", action="store_true", help="skip the learned/Morton comparison legs")
+    ap.add_argument("--no-extras", action="store_true",
+                    help="headline line only: skip the clustered (C3), index-form (C4) and serving (C5) sections")
+    ap.add_argument("--extra-steps", type=int, default=3,
+                    help="timed steps per leg of the C3/C4 sections of the headline line (at most --steps)")
     ap.add_argument("--overlap", action="store_true",
                     help="let index builds' kernels run beside the counts (default: after them; copies overlap)")
     ap.add_argument("--particles", type=int, default=None, help="override particles per file (profiling cases)")
@@ -1092,6 +1325,13 @@ def main():
             print(json.dumps(line), flush=True)
         return
     line = run_ours(args, w, dist, rank, world, local)
+    # configs 3-5 ride on the headline line at one GPU (replica runs time the headline only)
+    if not args.no_extras and world == 1:
+        extras, parity = run_extras(args, dist, rank, world, local, K=max(1, min(args.steps, args.extra_steps)),
+                                    W=3, small=args.small)
+        line.update(extras)
+        if parity:
+            line["parity_at_scale"] = {**(line.get("parity_at_scale") or {}), **parity}
     dist_close(dist)
     if rank == 0:
         print(json.dumps(line), flush=True)

@@ -296,8 +296,28 @@ int sjcs_query_read_counts_async(sjcs_ctx *ctx, sjcs_query *q, uint64_t *counts)
  * host memory (returns at once when none is pending). */
 int sjcs_query_wait_read(sjcs_query *q);
 /* Device pointer to the query's uint32 accumulators [nhalos][nrads] in the
- * order the halos were given (valid until sjcs_query_destroy). */
+ * order the halos were given (valid until sjcs_query_destroy).  They hold the
+ * counts since the query's last fold (sjcs_query_folds; with no fold, all of
+ * them). */
 int sjcs_query_device_counts(const sjcs_query *q, uint32_t **d_counts);
+/* The reference accumulates unsigned 64-bit counts over any number of
+ * particle files (ulong_t counts[], src/astr_rcount/main.c:651).  A query
+ * accumulates on the device in uint32 and keeps an upper bound of what its
+ * counts since the last fold can hold (each sjcs_query_count or step launch
+ * adds n, or 8n for periodic queries with R >= 499, whose particles can lie in
+ * several images' boxes); before a call could carry an accumulator past the
+ * fold limit, the query adds the uint32 accumulators into 64-bit device
+ * totals and clears them (a fold).  Read-backs return the 64-bit totals, so
+ * counts never wrap.  A single call that could add more than the limit by
+ * itself (more than 2^32 - 1 particles, or 2^29 with R >= 499) fails with
+ * SJCS_ERR_INVALID.
+ * sjcs_query_set_fold_limit lowers the limit (default and maximum 2^32 - 1;
+ * at least 1): folds then happen sooner, with the same results -- a test
+ * hook that exercises the fold on small inputs.  sjcs_query_folds gives the
+ * number of folds since creation or the last reset.  Neither has a
+ * counterpart in the reference. */
+int sjcs_query_set_fold_limit(sjcs_ctx *ctx, sjcs_query *q, uint64_t limit);
+int sjcs_query_folds(const sjcs_query *q, uint32_t *out);
 /* Zero the accumulators and the timing history (start a new run over the
  * same halos). */
 int sjcs_query_reset(sjcs_ctx *ctx, sjcs_query *q);
@@ -365,7 +385,10 @@ int sjcs_server_create(sjcs_ctx *ctx, sjcs_index *const *indexes, int nindexes,
  * completes, out_counts (host, uint32 [nhalos][nrads], pinned or not) holds
  * its counts.  Both buffers must stay valid until sjcs_server_wait returns.
  * Returns at once with a ticket; SJCS_ERR_NOMEM if the request alone needs
- * more device memory than the budget. */
+ * more device memory than the budget.  The counts are uint32: a request whose
+ * counts could exceed 2^32 - 1 (the server's indexes hold more than 2^32 - 1
+ * particles together, or 2^29 for periodic radius tables with R >= 499; see
+ * sjcs_query_set_fold_limit) fails with SJCS_ERR_INVALID. */
 int sjcs_server_submit(sjcs_server *srv, const float *halo_xyz, size_t stride_bytes, uint64_t nhalos,
                        const float *r2, int nrads, int flags, uint32_t *out_counts, uint64_t *ticket);
 /* Block until the ticket's request has completed; info (may be NULL) gets its
@@ -429,8 +452,13 @@ int sjcs_multi_range_count(sjcs_ctx *ctx, const sjcs_index *idx,
  * limits above are rejected with SJCS_ERR_INVALID.  The first call on a
  * device (that device current) looks up the array's address with
  * cudaGetSymbolAddress; make that first call before any stream capture.
+ * Under lazy module loading (the CUDA default since 12.2) that first call is
+ * also when the driver creates the array on the device, so make it before a
+ * framework reserves the device's memory (or set CUDA_MODULE_LOADING=EAGER).
  * All calls share the array, so calls that overlap on the GPU race: keep
- * them on one stream.  Counts equal those of sjcs_query_count. */
+ * them on one stream.  Counts equal those of sjcs_query_count; each call
+ * adds at most n (8n for periodic tables with R >= 499) to an accumulator,
+ * and keeping d_counts below 2^32 across calls is the caller's part. */
 int sjcs_count_noalloc(const float *d_xyz, uint64_t n,
                        const float *d_halo_xyz, size_t stride_bytes, uint64_t nhalos,
                        const float *r2, int nrads, int flags,

@@ -100,7 +100,8 @@ int sjcs_gen_face_halos(uint32_t seed, uint64_t n, uint64_t id0, float margin, s
 /* Clustered particles: nclumps isotropic Gaussian clumps (centres uniform in
  * the box, sigma log-uniform in [sig_lo, sig_hi], weights lognormal(0, wsig)
  * normalised) hold frac_clumped of the particles, the rest uniform; wrapped
- * into [0,1000).  One MT stream per call. */
+ * into [0,1000).  Blocks of 2^20 particles draw from their own MT streams
+ * (seeded from seed and the block number) on parallel threads. */
 int sjcs_gen_clustered_particles(uint32_t seed, uint64_t n, uint32_t nclumps, double sig_lo, double sig_hi,
                                  double wsig, double frac_clumped, uint32_t clump_seed, float *out);
 /* Clustered halos: frac_at_clumps of them at clump centres (same clump_seed as

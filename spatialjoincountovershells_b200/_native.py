@@ -133,6 +133,8 @@ _SIGS = {
     "sjcs_query_read_counts_async": (_c.c_int, [_vp, _vp, _vp]),
     "sjcs_query_wait_read": (_c.c_int, [_vp]),
     "sjcs_query_device_counts": (_c.c_int, [_vp, _pp]),
+    "sjcs_query_set_fold_limit": (_c.c_int, [_vp, _vp, _u64]),
+    "sjcs_query_folds": (_c.c_int, [_vp, _c.POINTER(_c.c_uint32)]),
     "sjcs_query_reset": (_c.c_int, [_vp, _vp]),
     "sjcs_query_timing": (_c.c_int, [_vp, _c.POINTER(sjcs_timing)]),
     "sjcs_query_destroy": (_c.c_int, [_vp]),
@@ -559,6 +561,17 @@ class Query:
 
     def reset(self) -> None:
         _check(lib().sjcs_query_reset(self.ctx._h, self._h))
+
+    def set_fold_limit(self, limit: int) -> "Query":
+        """Fold the u32 device accumulators into the 64-bit totals once they could pass `limit`."""
+        _check(lib().sjcs_query_set_fold_limit(self.ctx._h, self._h, int(limit)))
+        return self
+
+    @property
+    def folds(self) -> int:
+        v = _c.c_uint32()
+        _check(lib().sjcs_query_folds(self._h, _c.byref(v)))
+        return int(v.value)
 
     def set_schedule(self, mode: int = SCHED_AUTO, piece: int = 0, max_pieces: int = 0, single: int = 0) -> "Query":
         sc = sjcs_schedule(mode, piece, max_pieces, single)

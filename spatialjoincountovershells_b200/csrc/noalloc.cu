@@ -10,13 +10,17 @@
 // file-scope __device__ array (SJCS_NOALLOC_SCRATCH_BYTES, about 9.3 MB),
 // plus the caller's own input and output buffers.
 //
-// Every GPU that loads this library holds that array until the process exits.
-// All calls share it and it keeps the last call's contents, so calls that
-// overlap on the GPU (two streams, two host threads) race and must be
+// Every GPU that loads this library's module holds that array until the
+// process exits.  With lazy module loading (the CUDA default since 12.2) the
+// module, and with it the array, is loaded on a device by the first call made
+// while that device is current -- its cudaGetSymbolAddress -- so that first
+// call is when the driver sets the 9.3 MB aside: make it before a framework
+// reserves the device's memory, or set CUDA_MODULE_LOADING=EAGER to load it
+// with the library.  Make that first call before any stream capture too.
+// All calls share the array and it keeps the last call's contents, so calls
+// that overlap on the GPU (two streams, two host threads) race and must be
 // serialised by the caller; the only state that must start at zero (the
-// cell-table gap counter) is cleared by each call.  The array's address on a
-// device is taken with cudaGetSymbolAddress by the first call made while that
-// device is current; make that first call before any stream capture.
+// cell-table gap counter) is cleared by each call.
 #include <cmath>
 #include <cstring>
 #include <mutex>
@@ -75,6 +79,15 @@ int scratch_address(unsigned char** out) {
     return SJCS_OK;
 }
 
+// The padded radius table travels as a kernel argument (copied at launch),
+// so no host buffer has to outlive the call.
+struct R2Table {
+    float v[kNR];
+};
+__global__ void k_put_r2(R2Table t, int pad, float* __restrict__ out) {
+    for (int i = threadIdx.x; i < pad; i += blockDim.x) out[i] = t.v[i];
+}
+
 __global__ void k_pack_halos(const char* __restrict__ base, size_t stride, uint64_t nh, float4* __restrict__ out) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nh) return;
@@ -110,18 +123,20 @@ extern "C" int sjcs_count_noalloc(const float* d_xyz, uint64_t n, const float* d
     int rc = scratch_address(&base);
     if (rc) return rc;
 
-    // radius table, as sjcs_query_create builds it (binary-search binning)
-    float tab[kNR];
+    // radius table, as sjcs_query_create builds it (binary-search binning),
+    // written by a kernel that receives it by value
+    R2Table tab;
     int pad = 1;
     while (pad < nrads) pad <<= 1;
     bool mono = true;
-    for (int i = 0; i < pad; ++i) tab[i] = i < nrads ? r2[i] : INFINITY;
+    for (int i = 0; i < pad; ++i) tab.v[i] = i < nrads ? r2[i] : INFINITY;
     for (int i = 0; i < nrads; ++i) {
         if (std::isnan(r2[i])) mono = false;
         if (i + 1 < nrads && !(r2[i] <= r2[i + 1])) mono = false;
     }
     float* d_r2 = reinterpret_cast<float*>(base + kOffR2);
-    SJCS_CUDA_TRY(cudaMemcpyAsync(d_r2, tab, (size_t)pad * sizeof(float), cudaMemcpyHostToDevice, s));
+    k_put_r2<<<1, kNR, 0, s>>>(tab, pad, d_r2);
+    SJCS_LAUNCH_CHECK();
 
     // the grid index, in the scratch array
     const float R = (float)std::sqrt((double)r2[nrads - 1]);

@@ -292,6 +292,15 @@ int sjcs_server_submit(sjcs_server* srv, const float* halo_xyz, size_t stride_by
     if (stride_bytes < 12 || stride_bytes % 4) return fail(SJCS_ERR_INVALID, "stride_bytes must be a multiple of 4 and >= 12");
     if (nhalos > 0xffffffffull) return fail(SJCS_ERR_INVALID, "too many halos");
     if (flags & ~SJCS_QUERY_PERIODIC) return fail(SJCS_ERR_INVALID, "unknown query flags 0x%x", flags);
+    {
+        // the request's counts are summed over every index into uint32
+        uint64_t bound = 0;
+        for (const sjcs_index* ix : srv->idx) bound += count_call_bound(flags, r2[nrads - 1], ix->n);
+        if (bound > 0xffffffffull)
+            return fail(SJCS_ERR_INVALID,
+                        "the request's counts could reach %llu, beyond its uint32 output; serve fewer particles",
+                        (unsigned long long)bound);
+    }
     Request* r = new (std::nothrow) Request();
     if (!r) return fail(SJCS_ERR_NOMEM, "out of host memory");
     r->halo_xyz = halo_xyz;

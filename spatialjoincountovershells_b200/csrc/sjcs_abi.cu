@@ -44,9 +44,22 @@ int fail(int code, const char* fmt, ...) {
 
 namespace {
 
-__global__ void k_widen_u32_u64(const uint32_t* __restrict__ in, uint64_t m, unsigned long long* __restrict__ out) {
+// out = the 64-bit totals: the u32 accumulators plus, after a fold, the
+// folded part (folded == nullptr: none yet).
+__global__ void k_widen_u32_u64(const uint32_t* __restrict__ in, uint64_t m,
+                                const unsigned long long* __restrict__ folded, unsigned long long* __restrict__ out) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) out[i] = in[i];
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride)
+        out[i] = (unsigned long long)in[i] + (folded ? folded[i] : 0ull);
+}
+
+// One fold: the 64-bit totals take the u32 accumulators, which restart at 0.
+__global__ void k_fold_counts(uint32_t* __restrict__ c32, uint64_t m, unsigned long long* __restrict__ c64) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < m; i += stride) {
+        c64[i] += c32[i];
+        c32[i] = 0u;
+    }
 }
 
 __global__ void k_fill_f32(float* __restrict__ p, uint64_t m, float v) {
@@ -208,12 +221,40 @@ cudaError_t after_reads(const sjcs_query* q, cudaStream_t s) {
     return q->read_queued ? cudaStreamWaitEvent(s, q->ev_d1, 0) : cudaSuccess;
 }
 
+// Before a count call that can add up to `add` to an accumulator: fold the
+// u32 accumulators into the 64-bit totals (on stream s) if the call could
+// otherwise carry one past q->fold_limit.  Called after after_reads(q, s).
+int fold_before_count(sjcs_ctx* ctx, sjcs_query* q, uint64_t add, cudaStream_t s) {
+    if (add > q->fold_limit)
+        return fail(SJCS_ERR_INVALID,
+                    "one count call could add %llu to a 32-bit accumulator (limit %llu): use indexes of fewer "
+                    "particles",
+                    (unsigned long long)add, (unsigned long long)q->fold_limit);
+    if (q->bound + add <= q->fold_limit) {
+        q->bound += add;
+        return SJCS_OK;
+    }
+    const uint64_t m = q->nhalos * (uint64_t)q->nrads;
+    if (m) {
+        if (!q->counts64) {
+            SJCS_CUDA_TRY(cudaMallocAsync(&q->counts64, m * sizeof(unsigned long long), s));
+            SJCS_CUDA_TRY(cudaMemsetAsync(q->counts64, 0, m * sizeof(unsigned long long), s));
+        }
+        k_fold_counts<<<ctx->num_sms * 8, 256, 0, s>>>(q->counts, m, q->counts64);
+        SJCS_LAUNCH_CHECK();
+    }
+    ++q->folds;
+    q->bound = add;
+    return SJCS_OK;
+}
+
 void free_query(sjcs_query* q) {
     if (!q) return;
     cudaStream_t s = q->ctx->s_count;
     after_reads(q, s);
     if (q->halos) cudaFreeAsync(q->halos, s);
     if (q->counts) cudaFreeAsync(q->counts, s);
+    if (q->counts64) cudaFreeAsync(q->counts64, s);
     if (q->d_r2) cudaFreeAsync(q->d_r2, s);
     if (q->d_lut) cudaFreeAsync(q->d_lut, s);
     cudaStreamSynchronize(s);
@@ -420,6 +461,7 @@ struct sjcs_step {
     cudaEvent_t ev_pre, ev0, ev1;
     size_t kernels;  // kernel nodes in the graph
     bool launched;
+    uint64_t n;      // particles per launch
 };
 
 namespace sjcs {
@@ -990,6 +1032,8 @@ int sjcs_query_count(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx) {
     cudaStream_t s = ctx->s_count;
     SJCS_CUDA_TRY(cudaStreamWaitEvent(s, idx->ev_ready, 0));
     SJCS_CUDA_TRY(after_reads(q, s));
+    rc = fold_before_count(ctx, q, count_call_bound(q->flags, q->r2max, idx->n), s);
+    if (rc) return rc;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     SJCS_CUDA_TRY(cudaEventCreate(&e0));
     SJCS_CUDA_TRY(cudaEventCreate(&e1));
@@ -1027,6 +1071,7 @@ int sjcs_step_create(sjcs_ctx* ctx, sjcs_query* q, const float* host_xyz, uint64
     st->magic = kStepMagic;
     st->ctx = ctx;
     st->q = q;
+    st->n = n;
     cudaEventCreate(&st->ev_pre);
     cudaEventCreate(&st->ev0);
     cudaEventCreate(&st->ev1);
@@ -1090,6 +1135,10 @@ int sjcs_step_launch(sjcs_ctx* ctx, sjcs_step* st) {
     int rc = set_device(ctx);
     if (rc) return rc;
     std::lock_guard<std::mutex> lk(ctx->mu);
+    // the 32-bit accumulators are folded first if this file could overflow them
+    SJCS_CUDA_TRY(after_reads(st->q, ctx->s_count));
+    rc = fold_before_count(ctx, st->q, count_call_bound(st->q->flags, st->q->r2max, st->n), ctx->s_count);
+    if (rc) return rc;
     // after everything queued so far on both streams (halo preparation,
     // earlier counts and read-backs of the query)
     SJCS_CUDA_TRY(cudaEventRecord(st->ev_pre, ctx->s_count));
@@ -1239,7 +1288,7 @@ int sjcs_query_read_counts(sjcs_ctx* ctx, sjcs_query* q, uint64_t* counts, int a
     unsigned long long* wide = nullptr;
     SJCS_CUDA_TRY(scr.alloc(&wide, m * sizeof(uint64_t)));
     cudaEventRecord(q->ev_d0, s);
-    k_widen_u32_u64<<<ctx->num_sms * 8, 256, 0, s>>>(q->counts, m, wide);
+    k_widen_u32_u64<<<ctx->num_sms * 8, 256, 0, s>>>(q->counts, m, q->counts64, wide);
     SJCS_LAUNCH_CHECK();
     if (!accumulate && is_pinned(counts)) {
         SJCS_CUDA_TRY(cudaMemcpyAsync(counts, wide, m * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
@@ -1305,7 +1354,7 @@ int sjcs_query_read_counts_async(sjcs_ctx* ctx, sjcs_query* q, uint64_t* counts)
     unsigned long long* wide = nullptr;
     SJCS_CUDA_TRY(scr.alloc(&wide, m * sizeof(uint64_t)));
     SJCS_CUDA_TRY(cudaEventRecord(q->ev_d0, s));
-    k_widen_u32_u64<<<ctx->num_sms * 8, 256, 0, s>>>(q->counts, m, wide);
+    k_widen_u32_u64<<<ctx->num_sms * 8, 256, 0, s>>>(q->counts, m, q->counts64, wide);
     SJCS_LAUNCH_CHECK();
     SJCS_CUDA_TRY(cudaMemcpyAsync(counts, wide, m * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
     SJCS_CUDA_TRY(cudaEventRecord(q->ev_d1, s));
@@ -1338,8 +1387,27 @@ int sjcs_query_reset(sjcs_ctx* ctx, sjcs_query* q) {
     const uint64_t m = q->nhalos * (uint64_t)q->nrads;
     SJCS_CUDA_TRY(after_reads(q, ctx->s_count));
     if (m) SJCS_CUDA_TRY(cudaMemsetAsync(q->counts, 0, m * sizeof(uint32_t), ctx->s_count));
+    if (m && q->counts64) SJCS_CUDA_TRY(cudaMemsetAsync(q->counts64, 0, m * sizeof(unsigned long long), ctx->s_count));
     SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_count));
+    q->bound = 0;
+    q->folds = 0;
     clear_count_events(q);
+    return SJCS_OK;
+}
+
+int sjcs_query_set_fold_limit(sjcs_ctx* ctx, sjcs_query* q, uint64_t limit) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_query(q) || q->ctx != ctx) return fail(SJCS_ERR_STATE, "query does not belong to this context");
+    if (limit < 1 || limit > 0xffffffffull)
+        return fail(SJCS_ERR_INVALID, "the fold limit must lie in [1, 2^32 - 1] (got %llu)", (unsigned long long)limit);
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    q->fold_limit = limit;
+    return SJCS_OK;
+}
+
+int sjcs_query_folds(const sjcs_query* q, uint32_t* out) {
+    if (!valid_query(q) || !out) return fail(SJCS_ERR_INVALID, "invalid argument");
+    *out = q->folds;
     return SJCS_OK;
 }
 

@@ -12,6 +12,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <cmath>
 #include <cstdint>
 #include <cstdio>
 #include <map>
@@ -184,9 +185,29 @@ struct sjcs_query {
     bool read_queued = false;     // an asynchronous read ended at ev_d1 (maybe still running)
     float last_d2h_ms;
     sjcs_schedule sched;  // count schedule (SJCS_SCHED_AUTO by default)
+    // 64-bit totals.  The u32 accumulators hold the counts since the last
+    // fold; before a count call could push one of them past fold_limit, the
+    // query adds them into counts64 (allocated at the first fold) and clears
+    // them, so the totals never wrap, whatever the number of files.
+    unsigned long long* counts64 = nullptr;
+    uint64_t bound = 0;                    // upper bound of any u32 accumulator since the last fold
+    uint64_t fold_limit = 0xffffffffull;   // largest value a u32 accumulator may reach
+    uint32_t folds = 0;
 };
 
 namespace sjcs {
+// Largest amount one count of n particles can add to a single (halo, shell)
+// accumulator.  A particle is counted at most once per periodic image, and
+// it can lie inside two images' query boxes only when a box is at least 1000
+// wide (R >= 500; 499 leaves room for the fp32 rounding of the box bounds),
+// so below that every particle counts at most once.  Non-periodic queries
+// search one image.
+inline uint64_t count_call_bound(int flags, float r2max, uint64_t n) {
+    const float R = (float)std::sqrt((double)r2max);
+    const bool multi = (flags & SJCS_QUERY_PERIODIC) && !(R < 499.0f);  // NaN R: assume the worst
+    return multi ? 8 * n : n;
+}
+
 constexpr uint32_t kCtxMagic = 0x534a4358u;    // "SJCX"
 constexpr uint32_t kIndexMagic = 0x534a4958u;  // "SJIX"
 constexpr uint32_t kQueryMagic = 0x534a5158u;  // "SJQX"

@@ -307,30 +307,118 @@ static float wrap1000(double v)
     return (float)v;
 }
 
+/* The clustered generators draw each block of 2^20 items from its own MT19937
+ * stream (seeded from the call's seed and the block number), so the blocks
+ * are generated by parallel threads and the output does not depend on the
+ * number of threads. */
+#define GEN_BLOCK (1u << 20)
+
+static uint32_t block_seed(uint32_t seed, uint64_t b)
+{
+    return seed * 2654435761u + (uint32_t)(b + 1) * 0x9e3779b9u;
+}
+
+typedef struct GenJob {
+    const Clumps *c;
+    uint32_t seed;
+    uint64_t n, id0;
+    double frac, jitter;
+    float *pts;
+    sjcs_halo *halos;
+    uint64_t b0, b1; /* blocks of this job */
+} GenJob;
+
+static void *particle_job(void *arg)
+{
+    GenJob *j = arg;
+    uint64_t b, i;
+    for (b = j->b0; b < j->b1; ++b) {
+        sjcs_mt s;
+        const uint64_t lo = b * GEN_BLOCK, hi = lo + GEN_BLOCK < j->n ? lo + GEN_BLOCK : j->n;
+        sjcs_mt_seed(&s, block_seed(j->seed, b));
+        for (i = lo; i < hi; ++i) {
+            float *p = j->pts + 3 * i;
+            if (mt_real2(&s) < j->frac) {
+                uint32_t k = pick_clump(j->c, mt_real2(&s));
+                p[0] = wrap1000(j->c->cx[k] + j->c->sig[k] * mt_normal(&s));
+                p[1] = wrap1000(j->c->cy[k] + j->c->sig[k] * mt_normal(&s));
+                p[2] = wrap1000(j->c->cz[k] + j->c->sig[k] * mt_normal(&s));
+            } else {
+                p[0] = (float)(mt_real2(&s) * 1000.0);
+                p[1] = (float)(mt_real2(&s) * 1000.0);
+                p[2] = (float)(mt_real2(&s) * 1000.0);
+            }
+        }
+    }
+    return NULL;
+}
+
+static void *halo_job(void *arg)
+{
+    GenJob *j = arg;
+    uint64_t b, i;
+    for (b = j->b0; b < j->b1; ++b) {
+        sjcs_mt s;
+        const uint64_t lo = b * GEN_BLOCK, hi = lo + GEN_BLOCK < j->n ? lo + GEN_BLOCK : j->n;
+        sjcs_mt_seed(&s, block_seed(j->seed, b));
+        for (i = lo; i < hi; ++i) {
+            sjcs_halo *h = j->halos + i;
+            h->id = j->id0 + i;
+            h->mass = (float)(mt_real2(&s) * 1e12);
+            if (mt_real2(&s) < j->frac) {
+                /* halos sit at clump centres (uniform over clumps, not weighted) */
+                uint32_t k = (uint32_t)(sjcs_mt_u32(&s) % j->c->n);
+                h->point[0] = wrap1000(j->c->cx[k] + j->jitter * mt_normal(&s));
+                h->point[1] = wrap1000(j->c->cy[k] + j->jitter * mt_normal(&s));
+                h->point[2] = wrap1000(j->c->cz[k] + j->jitter * mt_normal(&s));
+            } else {
+                h->point[0] = (float)(mt_real2(&s) * 1000.0);
+                h->point[1] = (float)(mt_real2(&s) * 1000.0);
+                h->point[2] = (float)(mt_real2(&s) * 1000.0);
+            }
+        }
+    }
+    return NULL;
+}
+
+/* Run fn over the blocks of job proto on up to 64 threads. */
+static void run_blocks(GenJob proto, void *(*fn)(void *))
+{
+    GenJob jobs[64];
+    pthread_t th[64];
+    const uint64_t nb = (proto.n + GEN_BLOCK - 1) / GEN_BLOCK;
+    long hw = sysconf(_SC_NPROCESSORS_ONLN);
+    int T = hw < 1 ? 1 : (hw > 64 ? 64 : (int)hw), t;
+    if ((uint64_t)T > nb)
+        T = nb ? (int)nb : 1;
+    for (t = 0; t < T; ++t) {
+        jobs[t] = proto;
+        jobs[t].b0 = nb * t / T;
+        jobs[t].b1 = nb * (t + 1) / T;
+    }
+    for (t = 1; t < T; ++t)
+        pthread_create(&th[t], NULL, fn, &jobs[t]);
+    fn(&jobs[0]);
+    for (t = 1; t < T; ++t)
+        pthread_join(th[t], NULL);
+}
+
 int sjcs_gen_clustered_particles(uint32_t seed, uint64_t n, uint32_t nclumps, double sig_lo, double sig_hi,
                                  double wsig, double frac_clumped, uint32_t clump_seed, float *out)
 {
     Clumps c;
-    sjcs_mt s;
-    uint64_t i;
+    GenJob j;
     if (make_clumps(&c, nclumps, sig_lo, sig_hi, wsig, clump_seed) != 0) {
         free_clumps(&c);
         return -1;
     }
-    sjcs_mt_seed(&s, seed);
-    for (i = 0; i < n; ++i) {
-        float *p = out + 3 * i;
-        if (mt_real2(&s) < frac_clumped) {
-            uint32_t k = pick_clump(&c, mt_real2(&s));
-            p[0] = wrap1000(c.cx[k] + c.sig[k] * mt_normal(&s));
-            p[1] = wrap1000(c.cy[k] + c.sig[k] * mt_normal(&s));
-            p[2] = wrap1000(c.cz[k] + c.sig[k] * mt_normal(&s));
-        } else {
-            p[0] = (float)(mt_real2(&s) * 1000.0);
-            p[1] = (float)(mt_real2(&s) * 1000.0);
-            p[2] = (float)(mt_real2(&s) * 1000.0);
-        }
-    }
+    memset(&j, 0, sizeof(j));
+    j.c = &c;
+    j.seed = seed;
+    j.n = n;
+    j.frac = frac_clumped;
+    j.pts = out;
+    run_blocks(j, particle_job);
     free_clumps(&c);
     return 0;
 }
@@ -340,28 +428,20 @@ int sjcs_gen_clustered_halos(uint32_t seed, uint64_t n, uint64_t id0, uint32_t n
                              uint32_t clump_seed, sjcs_halo *out)
 {
     Clumps c;
-    sjcs_mt s;
-    uint64_t i;
+    GenJob j;
     if (make_clumps(&c, nclumps, sig_lo, sig_hi, wsig, clump_seed) != 0) {
         free_clumps(&c);
         return -1;
     }
-    sjcs_mt_seed(&s, seed);
-    for (i = 0; i < n; ++i) {
-        out[i].id = id0 + i;
-        out[i].mass = (float)(mt_real2(&s) * 1e12);
-        if (mt_real2(&s) < frac_at_clumps) {
-            /* halos sit at clump centres (uniform over clumps, not weighted) */
-            uint32_t k = (uint32_t)(sjcs_mt_u32(&s) % c.n);
-            out[i].point[0] = wrap1000(c.cx[k] + jitter * mt_normal(&s));
-            out[i].point[1] = wrap1000(c.cy[k] + jitter * mt_normal(&s));
-            out[i].point[2] = wrap1000(c.cz[k] + jitter * mt_normal(&s));
-        } else {
-            out[i].point[0] = (float)(mt_real2(&s) * 1000.0);
-            out[i].point[1] = (float)(mt_real2(&s) * 1000.0);
-            out[i].point[2] = (float)(mt_real2(&s) * 1000.0);
-        }
-    }
+    memset(&j, 0, sizeof(j));
+    j.c = &c;
+    j.seed = seed;
+    j.n = n;
+    j.id0 = id0;
+    j.frac = frac_at_clumps;
+    j.jitter = jitter;
+    j.halos = out;
+    run_blocks(j, halo_job);
     free_clumps(&c);
     round_all(out, n, 0);
     return 0;
