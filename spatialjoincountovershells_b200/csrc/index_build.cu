@@ -1,4 +1,7 @@
-// Plain (grid) index build for one particle file.
+// Plain (grid) index build for one particle file: the radix build below,
+// used for grids of more than 2^28 cells and by the allocation-free entry
+// point; every other grid index is built by the two-pass bucket build
+// (bucket_build.cu).
 //
 // Replaces the STR bulk load of the reference (MakeTreeWithSameThreadPoolArraySTR,
 // src/objects/ArraySTR/Build.c:845-963: per level, LSD radix sorts on the
@@ -199,11 +202,28 @@ int fill_cell_table(const uint32_t* sorted_cells, uint64_t n, uint64_t ncells, u
 
 int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGeom& g,
                      sjcs_index* idx, cudaStream_t s) {
-    (void)ctx;
     idx->geom = g;
     const uint64_t nalloc = n ? n : 1;
     SJCS_CUDA_TRY(cudaMallocAsync(&idx->pts, nalloc * sizeof(float4), s));
     SJCS_CUDA_TRY(cudaMallocAsync(&idx->cell_start, (g.ncells + 1) * sizeof(uint32_t), s));
+    if (n == 0) {
+        SJCS_CUDA_TRY(cudaMemsetAsync(idx->cell_start, 0, (g.ncells + 1) * sizeof(uint32_t), s));
+        return SJCS_OK;
+    }
+    if (bucket_build_eligible(g, n)) {
+        const BucketBuildSizes z = bucket_build_sizes(g, n, ctx->num_sms);
+        BucketBuildBuffers bb{};
+        bb.pts = idx->pts;
+        bb.cell_start = idx->cell_start;
+        StreamScratch scr(s);  // freed (stream-ordered) on every return path
+        SJCS_CUDA_TRY(scr.alloc(&bb.part, z.part * sizeof(uint4)));
+        SJCS_CUDA_TRY(scr.alloc(&bb.hist, z.hist * sizeof(uint32_t)));
+        SJCS_CUDA_TRY(scr.alloc(&bb.partials, z.partials * sizeof(uint32_t)));
+        SJCS_CUDA_TRY(scr.alloc(&bb.heavy_count, sizeof(uint32_t)));
+        SJCS_CUDA_TRY(scr.alloc(&bb.heavy_ids, z.max_heavy * sizeof(uint32_t)));
+        SJCS_CUDA_TRY(scr.alloc(&bb.cursors, z.cursors * sizeof(uint32_t)));
+        return build_grid_bucketed(d_xyz, n, g, ctx->num_sms, bb, s);
+    }
 
     GridBuildBuffers b{};
     b.pts = idx->pts;
