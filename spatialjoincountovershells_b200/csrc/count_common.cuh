@@ -32,6 +32,8 @@ struct CountParams {
     int periodic;
     int prune;
     uint32_t* __restrict__ counts;
+    uint32_t* err;                   // wait-error flag (host-mapped); null: no staged kernel
+    uint32_t stage_extra_bytes;      // 0 (a test hook adds bytes no copy delivers)
 };
 
 __device__ __forceinline__ float edge_margin(float v) { return 1e-3f + 2e-6f * fabsf(v); }

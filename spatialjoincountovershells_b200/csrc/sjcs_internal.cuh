@@ -131,6 +131,11 @@ struct sjcs_ctx {
     std::mutex ring_mu;
     char* ring = nullptr;
     std::vector<cudaEvent_t> ring_ev;
+    // Set (to 1) by a kernel whose bounded wait gave up; page-locked and
+    // mapped, so the host reads it after a wait without a copy.
+    uint32_t* h_err = nullptr;
+    uint32_t* d_err = nullptr;  // device address of *h_err
+    uint32_t stage_extra = 0;   // test hook: bytes the count kernel's staged copies over-expect
 };
 
 namespace sjcs {
@@ -211,6 +216,10 @@ inline uint64_t count_call_bound(int flags, float r2max, uint64_t n) {
 constexpr uint32_t kCtxMagic = 0x534a4358u;    // "SJCX"
 constexpr uint32_t kIndexMagic = 0x534a4958u;  // "SJIX"
 constexpr uint32_t kQueryMagic = 0x534a5158u;  // "SJQX"
+
+// sjcs_abi.cu: SJCS_ERR_TIMEOUT (and the flag cleared) if one of ctx's
+// kernels gave up a bounded wait since the last check, else SJCS_OK.
+int wait_errors(sjcs_ctx* ctx);
 
 // index_build.cu
 int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGeom& g,
