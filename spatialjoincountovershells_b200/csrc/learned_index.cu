@@ -15,8 +15,9 @@
 //            prefix), the level-L cell of every particle and (learned kind)
 //            the full keys
 //   table    table[c] = first slot of level-L cell c (the plain offset table)
-//   train    (learned kind) root from kmin/kmax, exact leaf rank ranges,
-//            anchor + fp32 slope per leaf, per-leaf max error over all keys
+//   train    (learned kind) equal-population leaf rank ranges, a fitted
+//            fp32 slope and bias per leaf and its exact max error, the
+//            root's directory over the leaves' anchors
 //   judge    (learned kind, on request) the corrected model rank of every
 //            level-L cell boundary is compared with the table; any mismatch
 //            switches the count kernel to the table for this index
@@ -76,58 +77,117 @@ __global__ void k_root(const unsigned long long* __restrict__ keys, uint64_t n, 
     r.kmin = keys[0];
     r.kmax = keys[n - 1];
     uint32_t sh = 0;
-    while (((r.kmax - r.kmin) >> sh) >= kLeaves) ++sh;
+    while (((r.kmax - r.kmin) >> sh) >= (1ull << kDirBits)) ++sh;
     r.shift = sh;
     r.n = (uint32_t)n;
     *rt = r;
 }
 
-// first[j] = first rank whose key lies in leaf j or later (first[4096] = n).
-__global__ void k_leaf_bounds(const unsigned long long* __restrict__ keys, uint64_t n,
-                              const LearnedRoot* __restrict__ rt, uint32_t* __restrict__ first) {
-    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i > n) return;
-    const LearnedRoot r = *rt;
-    const int64_t jp = (i == 0) ? -1 : (int64_t)leaf_of(r, keys[i - 1]);
-    const int64_t jc = (i == n) ? (int64_t)kLeaves : (int64_t)leaf_of(r, keys[i]);
-    for (int64_t j = jp + 1; j <= jc; ++j) first[j] = (uint32_t)i;
+// first[j] = first rank of leaf j: the first occurrence of the key at rank
+// j*n/4096 (first[4096] = n), so every leaf holds about n/4096 keys and
+// equal keys share a leaf.
+__global__ void k_leaf_first(const unsigned long long* __restrict__ keys, uint64_t n, uint32_t* __restrict__ first) {
+    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j > kLeaves) return;
+    const uint64_t r = (uint64_t)j * n / kLeaves;
+    if (r >= n) {
+        first[j] = (uint32_t)n;
+        return;
+    }
+    const unsigned long long k = keys[r];
+    uint64_t lo = 0, hi = r;  // lower bound of k in keys[0, r]
+    while (lo < hi) {
+        const uint64_t mid = (lo + hi) >> 1;
+        if (keys[mid] < k) lo = mid + 1;
+        else hi = mid;
+    }
+    first[j] = (uint32_t)lo;
 }
 
-__global__ void k_leaf_fit(const unsigned long long* __restrict__ keys, const uint32_t* __restrict__ first,
-                           LearnedLeaf* __restrict__ leaves) {
-    const uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= kLeaves) return;
+template <class T>
+__device__ __forceinline__ T block_reduce(T v, T (*op)(T, T), T* sh) {
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    __syncthreads();  // sh is free (an earlier reduction may still be reading it)
+    if (lane == 0) sh[w] = v;
+    __syncthreads();
+    v = sh[0];
+    for (int k = 1; k < nw; ++k) v = op(v, sh[k]);
+    return v;
+}
+__device__ double dadd(double a, double b) { return a + b; }
+__device__ double dmin(double a, double b) { return fmin(a, b); }
+__device__ double dmax(double a, double b) { return fmax(a, b); }
+__device__ uint32_t umax(uint32_t a, uint32_t b) { return max(a, b); }
+
+// One block per leaf: least-squares slope of rank over key offset (double),
+// the bias that centres the extreme residuals of the fp32 prediction, and
+// the exact error bound of the final fp32 predictor.
+__global__ void __launch_bounds__(256) k_leaf_fit(const unsigned long long* __restrict__ keys, uint64_t n,
+                                                  const uint32_t* __restrict__ first,
+                                                  LearnedLeaf* __restrict__ leaves) {
+    __shared__ double shd[8];
+    __shared__ uint32_t shu[8];
+    const uint32_t j = blockIdx.x;
     LearnedLeaf lf{};
     lf.r0 = first[j];
     lf.r1 = first[j + 1];
-    if (lf.r1 > lf.r0) {
-        lf.anchor = keys[lf.r0];
-        const unsigned long long last = keys[lf.r1 - 1];
-        if (lf.r1 - lf.r0 >= 2 && last > lf.anchor)
-            lf.slope = (float)(lf.r1 - lf.r0 - 1) / __ull2float_rn(last - lf.anchor);
+    lf.anchor = lf.r0 < n ? keys[lf.r0] : ~0ull;
+    const uint32_t m = lf.r1 - lf.r0;
+    if (m >= 2) {
+        double sx = 0, sy = 0, sxx = 0, sxy = 0;
+        for (uint32_t i = lf.r0 + threadIdx.x; i < lf.r1; i += blockDim.x) {
+            const double x = (double)(keys[i] - lf.anchor), y = (double)(i - lf.r0);
+            sx += x;
+            sy += y;
+            sxx += x * x;
+            sxy += x * y;
+        }
+        sx = block_reduce(sx, dadd, shd);
+        sy = block_reduce(sy, dadd, shd);
+        sxx = block_reduce(sxx, dadd, shd);
+        sxy = block_reduce(sxy, dadd, shd);
+        const double var = sxx - sx * sx / m, cov = sxy - sx * sy / m;
+        double b = var > 0 ? cov / var : 0.0;
+        if (!(b >= 0) || !isfinite(b)) b = 0.0;
+        lf.slope = (float)b;
+        double lo = 1e300, hi = -1e300;
+        for (uint32_t i = lf.r0 + threadIdx.x; i < lf.r1; i += blockDim.x) {
+            const float x = __ull2float_rn(keys[i] - lf.anchor);
+            const double d = (double)(i - lf.r0) - (double)__fmul_rn(x, lf.slope);
+            lo = fmin(lo, d);
+            hi = fmax(hi, d);
+        }
+        lo = block_reduce(lo, dmin, shd);
+        hi = block_reduce(hi, dmax, shd);
+        lf.bias = (float)(0.5 * (lo + hi) + 0.5);  // + 0.5: truncation then rounds to nearest
+        uint32_t e = 0;
+        for (uint32_t i = lf.r0 + threadIdx.x; i < lf.r1; i += blockDim.x) {
+            const uint32_t P = leaf_predict(lf, keys[i]);
+            e = max(e, P > i ? P - i : i - P);
+        }
+        lf.err = block_reduce(e, umax, shu);
     }
-    leaves[j] = lf;
+    if (threadIdx.x == 0) leaves[j] = lf;
 }
 
-// err[leaf] = max |P(k_i) - i|, one warp-aggregated atomic per leaf run.
-__global__ void k_leaf_err(const unsigned long long* __restrict__ keys, uint64_t n,
-                           const LearnedRoot* __restrict__ rt, LearnedLeaf* __restrict__ leaves) {
+// dir[b] = number of leaves whose anchor is <= kmin + (b << shift), b <= 2^16.
+__global__ void k_leaf_dir(const LearnedLeaf* __restrict__ leaves, const LearnedRoot* __restrict__ rt,
+                           uint16_t* __restrict__ dir) {
+    const uint32_t b = blockIdx.x * blockDim.x + threadIdx.x;
+    if (b >= kDirEntries) return;
     const LearnedRoot r = *rt;
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t base = (uint64_t)blockIdx.x * blockDim.x; base < n; base += stride) {
-        const uint64_t i = base + threadIdx.x;
-        const bool valid = i < n;
-        uint32_t j = 0xffffffffu, e = 0;
-        if (valid) {
-            const unsigned long long k = keys[i];
-            j = leaf_of(r, k);
-            const uint32_t P = leaf_predict(leaves[j], k);
-            e = P > (uint32_t)i ? P - (uint32_t)i : (uint32_t)i - P;
-        }
-        const uint32_t peers = __match_any_sync(0xffffffffu, j);
-        const uint32_t m = __reduce_max_sync(peers, e);
-        if (valid && (threadIdx.x & 31) == (uint32_t)(__ffs(peers) - 1) && m) atomicMax(&leaves[j].err, m);
+    // kmax - kmin < 2^63 keeps shift <= 47, so b << shift (b <= 2^16) fits
+    const uint64_t off = (uint64_t)b << r.shift;
+    const unsigned long long q = off > r.kmax - r.kmin ? ~0ull : r.kmin + off;
+    uint32_t lo = 0, hi = kLeaves;  // upper bound of q among the anchors
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (leaves[mid].anchor <= q) lo = mid + 1;
+        else hi = mid;
     }
+    dir[b] = (uint16_t)min(lo, (uint32_t)kLeaves);
 }
 
 __global__ void k_leaf_stats(const LearnedLeaf* __restrict__ leaves, LearnedRoot* rt) {
@@ -211,10 +271,10 @@ int build_morton_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, int level,
     SJCS_CUDA_TRY(cudaMallocAsync(&idx->pts, nalloc * sizeof(float4), s));
     SJCS_CUDA_TRY(cudaMallocAsync(&idx->cell_start, (ncells + 1) * sizeof(uint32_t), s));
     if (learned) {
-        SJCS_CUDA_TRY(cudaMallocAsync(&idx->leaves, kLeaves * sizeof(LearnedLeaf), s));
+        SJCS_CUDA_TRY(cudaMallocAsync(reinterpret_cast<void**>(&idx->leaves), kModelBytes, s));
         SJCS_CUDA_TRY(cudaMallocAsync(&idx->root, sizeof(LearnedRoot), s));
         SJCS_CUDA_TRY(cudaMemsetAsync(idx->root, 0, sizeof(LearnedRoot), s));
-        SJCS_CUDA_TRY(cudaMemsetAsync(idx->leaves, 0, kLeaves * sizeof(LearnedLeaf), s));
+        SJCS_CUDA_TRY(cudaMemsetAsync(idx->leaves, 0, kModelBytes, s));
     }
     if (n == 0) {
         SJCS_CUDA_TRY(cudaMemsetAsync(idx->cell_start, 0, (ncells + 1) * sizeof(uint32_t), s));
@@ -269,12 +329,12 @@ int build_morton_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, int level,
 
     k_root<<<1, 1, 0, s>>>(keys, n, idx->root);
     SJCS_LAUNCH_CHECK();
-    k_leaf_bounds<<<(unsigned)((n + 1 + 255) / 256), 256, 0, s>>>(keys, n, idx->root, first);
+    k_leaf_first<<<(kLeaves + 1 + 255) / 256, 256, 0, s>>>(keys, n, first);
     SJCS_LAUNCH_CHECK();
-    k_leaf_fit<<<kLeaves / 256, 256, 0, s>>>(keys, first, idx->leaves);
+    k_leaf_fit<<<kLeaves, 256, 0, s>>>(keys, n, first, idx->leaves);
     SJCS_LAUNCH_CHECK();
-    const unsigned eblocks = (unsigned)std::min<uint64_t>((n + 255) / 256, 148ull * 16);
-    k_leaf_err<<<eblocks, 256, 0, s>>>(keys, n, idx->root, idx->leaves);
+    k_leaf_dir<<<(kDirEntries + 255) / 256, 256, 0, s>>>(idx->leaves, idx->root,
+                                                          reinterpret_cast<uint16_t*>(idx->leaves + kLeaves));
     SJCS_LAUNCH_CHECK();
     k_leaf_stats<<<1, 1024, 0, s>>>(idx->leaves, idx->root);
     SJCS_LAUNCH_CHECK();

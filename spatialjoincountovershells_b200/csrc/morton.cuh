@@ -12,14 +12,19 @@
 // HBM layout of a Morton index over n particles:
 //   pts[n]              float4 (x, y, z, level-10 prefix bits), sorted by key
 //   table[8^L + 1]      u32 plain offset table of the index's cell level L
-//   leaves[4096]        LearnedLeaf, root (one LearnedRoot)   (learned kind)
+//   leaves[4096]        LearnedLeaf, then the root's directory (2^16 + 1 u16),
+//   root                one LearnedRoot                         (learned kind)
 //
-// Rank model (learned kind): the root maps a key to leaf
-// j = (key - kmin) >> shift, the smallest shift that puts kmax in leaf 4095
-// (a linear root with slope 2^-shift, exact in integers).  Leaf j holds the
-// exact first rank r0 of its key range, the first key `anchor` and an fp32
-// slope; its prediction P(q) = r0 + min(trunc(fp32((q - anchor)) * slope), r1 - r0)
-// (P(q) = r0 for q <= anchor) is monotone in q.  Training records
+// Rank model (learned kind), in the manner of a radix spline: 4096 leaves of
+// equal population -- leaf j holds the ranks [r0_j, r1_j) with r0_j the first
+// rank of the key at rank j*n/4096 (so equal keys never straddle two leaves)
+// and covers the keys [anchor_j, anchor_{j+1}), anchor_j = key[r0_j].  The
+// root finds a key's leaf: a 2^16-entry directory over (key - kmin) >> shift
+// gives the few leaves whose anchors can precede the key, and a short binary
+// search over those anchors picks the last one <= key.  Leaf j predicts
+//     P(q) = r0 + min(trunc(clamp(fp32(fp32(q - anchor) * slope) + bias)), r1 - r0),
+// slope and bias fitted to the leaf's keys (least squares, then the bias
+// centred on the extreme residuals); P is monotone in q.  Training records
 // err = max over the leaf's keys k_i of |P(k_i) - i|.  For a query key q in
 // leaf j the true lower bound t satisfies
 //     t < r1  =>  P(q) <= P(k_t) <= t + err
@@ -39,17 +44,24 @@ constexpr uint32_t kLeaves = 1u << kLeafBits;  // 4096 leaves
 constexpr int kPrefixLevel = 10;               // pts[i].w holds the key's top 30 bits
 constexpr int kMaxMortonLevel = 10;
 
+constexpr int kDirBits = 16;
+constexpr uint32_t kDirEntries = (1u << kDirBits) + 1u;
+
 struct LearnedLeaf {
-    unsigned long long anchor;  // first key of the leaf (0 if empty)
+    unsigned long long anchor;  // first key of the leaf (~0 for an empty leaf at the end)
     uint32_t r0, r1;            // exact rank range of the leaf's keys
     float slope;                // ranks per key unit
+    float bias;                 // ranks added before truncation
     uint32_t err;               // max |P(k_i) - i| over the leaf's keys
+    uint32_t pad_;
 };
-static_assert(sizeof(LearnedLeaf) == 24, "leaf records are 24 bytes");
+static_assert(sizeof(LearnedLeaf) == 32, "leaf records are 32 bytes");
+// bytes of the leaves and the root's directory (one allocation)
+constexpr size_t kModelBytes = kLeaves * sizeof(LearnedLeaf) + kDirEntries * sizeof(uint16_t);
 
 struct LearnedRoot {
     unsigned long long kmin, kmax;
-    uint32_t shift;
+    uint32_t shift;  // directory bucket of a key: (key - kmin) >> shift (< 2^16)
     uint32_t n;
     unsigned long long checked;     // cell boundaries compared with the table
     unsigned long long mismatches;  // lookups that disagreed (then the table is used)
@@ -79,13 +91,29 @@ __device__ __forceinline__ uint32_t morton_cell(uint32_t x, uint32_t y, uint32_t
     return spread3_10(x) | (spread3_10(y) << 1) | (spread3_10(z) << 2);
 }
 
-__device__ __forceinline__ uint32_t leaf_of(const LearnedRoot& rt, uint64_t key) {
-    return (uint32_t)((key - rt.kmin) >> rt.shift);
+__device__ __forceinline__ const uint16_t* model_dir(const LearnedLeaf* leaves) {
+    return reinterpret_cast<const uint16_t*>(leaves + kLeaves);
+}
+
+// Leaf of a key in [kmin, kmax]: the last leaf whose anchor is <= key.
+__device__ __forceinline__ uint32_t leaf_of(const LearnedRoot& rt, const LearnedLeaf* __restrict__ leaves,
+                                            uint64_t key) {
+    const uint16_t* dir = model_dir(leaves);
+    const uint32_t b = (uint32_t)((key - rt.kmin) >> rt.shift);
+    uint32_t lo = __ldg(dir + b), hi = __ldg(dir + b + 1);  // counts of anchors <= the bucket's ends
+    lo = lo ? lo - 1u : 0u;
+    hi = hi ? hi - 1u : 0u;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi + 1u) >> 1;
+        if (__ldg(&leaves[mid].anchor) <= key) lo = mid;
+        else hi = mid - 1u;
+    }
+    return lo;
 }
 
 __device__ __forceinline__ uint32_t leaf_predict(const LearnedLeaf& lf, uint64_t q) {
-    if (q <= lf.anchor) return lf.r0;
-    const float off = fminf(__fmul_rn(__ull2float_rn(q - lf.anchor), lf.slope), 4.0e9f);
+    const float x = __ull2float_rn(q - lf.anchor);  // q >= anchor
+    const float off = fminf(fmaxf(__fadd_rn(__fmul_rn(x, lf.slope), lf.bias), 0.0f), 4.0e9f);
     const uint32_t d = (uint32_t)off;  // off >= 0: truncation is floor
     const uint32_t span = lf.r1 - lf.r0;
     return lf.r0 + (d < span ? d : span);
@@ -98,7 +126,7 @@ __device__ __forceinline__ uint32_t learned_rank(const LearnedRoot& rt, const Le
                                                  const uint32_t* __restrict__ wpref, uint64_t q) {
     if (q <= rt.kmin) return 0u;
     if (q > rt.kmax) return rt.n;
-    const LearnedLeaf lf = leaves[leaf_of(rt, q)];
+    const LearnedLeaf lf = leaves[leaf_of(rt, leaves, q)];
     const uint32_t P = leaf_predict(lf, q);
     uint32_t lo = (P - lf.r0 > lf.err) ? P - lf.err : lf.r0;
     const uint64_t hi64 = (uint64_t)P + lf.err + 1ull;
@@ -131,7 +159,7 @@ __device__ __forceinline__ void learned_rank_n(const LearnedRoot& rt, const Lear
             lo[j] = hi[j] = rt.n;
             continue;
         }
-        const LearnedLeaf lf = leaves[leaf_of(rt, q[j])];
+        const LearnedLeaf lf = leaves[leaf_of(rt, leaves, q[j])];
         const uint32_t P = leaf_predict(lf, q[j]);
         lo[j] = (P - lf.r0 > lf.err) ? P - lf.err : lf.r0;
         const uint64_t h64 = (uint64_t)P + lf.err + 1ull;
