@@ -49,7 +49,6 @@ extern "C" {
 #define SJCS_ERR_CUDA      2  /* CUDA runtime error or no usable device */
 #define SJCS_ERR_NOMEM     3  /* device or pinned-host allocation failed */
 #define SJCS_ERR_STATE     4  /* object used with another context, or after destroy */
-#define SJCS_ERR_TIMEOUT   5  /* a bounded device-side wait gave up (error flag set) */
 
 /* index kinds */
 #define SJCS_INDEX_GRID     0 /* uniform cell grid: particles radix-sorted by cell, cell-offset table */
@@ -175,17 +174,6 @@ uint64_t sjcs_launch_counter(void);
  * backlog pipeline (src/astr_rcount/main.c:266-350) overlaps them because its
  * builds and searches use separate CPU threads. */
 int sjcs_ctx_set_overlap(sjcs_ctx *ctx, int overlap);
-/* Bounded waits.  The count kernel's static schedule stages each halo's
- * candidates in shared memory with bulk asynchronous copies and waits for
- * them with a bound of about 2^31 SM clocks (~1 s); a wait that gives up sets
- * the context's error flag and its warp stops counting.  sjcs_query_wait,
- * sjcs_query_read_counts, sjcs_query_wait_read, sjcs_step_wait and
- * sjcs_ctx_sync then return SJCS_ERR_TIMEOUT once (and clear the flag); a
- * serving request returns it as its status.  sjcs_ctx_set_wait_test is a test
- * hook: extra_bytes > 0 makes every staged copy expect that many bytes more
- * than it delivers, so its waits run out (0 restores normal operation).  No
- * counterpart in the reference. */
-int sjcs_ctx_set_wait_test(sjcs_ctx *ctx, uint32_t extra_bytes);
 
 /* ---- pinned host memory (for the driver's file reads) -------------------- */
 

@@ -96,7 +96,6 @@ _SIGS = {
     "sjcs_ctx_memory": (_c.c_int, [_vp, _c.POINTER(_u64), _c.POINTER(_u64)]),
     "sjcs_launch_counter": (_c.c_uint64, []),
     "sjcs_ctx_set_overlap": (_c.c_int, [_vp, _c.c_int]),
-    "sjcs_ctx_set_wait_test": (_c.c_int, [_vp, _c.c_uint32]),
     "sjcs_host_alloc": (_c.c_int, [_c.c_size_t, _pp]),
     "sjcs_host_free": (_c.c_int, [_vp]),
     "sjcs_index_build": (_c.c_int, [_vp, _vp, _u64, _c.POINTER(sjcs_index_opts), _pp]),

@@ -6,7 +6,7 @@
 // shape, and none depends on the order of the particles inside a cell, so
 // the index only has to group particles by cell and record where each cell
 // starts.  Cells are numbered x-fastest; a bucket is 2^L consecutive cell ids
-// (L = 14: ~17 rows of x cells of one z layer at the automatic grid).
+// (L = 13: ~8.7 rows of x cells of one z layer at the automatic grid).
 //
 //   k_bucket_hist     chunk c of the AoS input (S particles): per-bucket
 //                     particle counts -> hist[bucket][chunk]
@@ -14,19 +14,30 @@
 //                     chunk c's particles of bucket b go; hist[b][0] is the
 //                     start of bucket b
 //   k_bucket_scatter  chunk c again: each particle takes the next slot of its
-//                     bucket (shared-memory cursor, order inside a bucket is
-//                     free) and is written as (x, y, z, cell id)
-//   k_bucket_sort     one block per bucket: counts per cell in shared memory,
-//                     their exclusive scan gives the bucket's cell_start
-//                     entries, then every particle takes the next slot of its
-//                     cell and is written as a float4 into pts
+//                     bucket (shared-memory cursor; the order inside a bucket
+//                     is free) and is written as one 32-byte record
+//                     (x, y, z, cell id, padding) with a single 256-bit store
+//   k_bucket_sort     persistent, one block per SM walking the buckets: per
+//                     bucket, counts per cell in shared memory (the records
+//                     kept in shared memory too), their exclusive scan gives
+//                     the bucket's cell_start entries, then every particle
+//                     takes the next slot of its cell and is written as a
+//                     float4 into pts
 //   k_heavy_*         buckets of more than kHeavy particles (clustered data)
 //                     are left by k_bucket_sort to three grid-wide kernels
 //                     that do the same with global-memory counters, so no
 //                     bucket holds one block for long
 //
-// Per particle: 12 B read twice, 16 B written and read (plus an L2 re-read),
-// 16 B written; per cell 4 B.  No block waits on another block.
+// Why 32-byte records: the scatter sends every particle to one of ~16k
+// buckets, so consecutive records of a bucket slice arrive far apart in time.
+// A 16-byte record leaves its 32-byte DRAM sector half written; when L2
+// evicts it before the other half arrives, the memory controller reads the
+// sector back to merge it.  A record that fills its sector is written whole.
+// The sort kernel keeps few buckets in flight (one per SM), so its scattered
+// 16-byte writes complete their lines in L2.
+//
+// Per particle: 12 B read twice, 32 B written and read once, 16 B written;
+// per cell 4 B.  No block waits on another block.
 #include <algorithm>
 
 #include "sjcs_internal.cuh"
@@ -34,12 +45,20 @@
 namespace sjcs {
 namespace {
 
-constexpr int kLocalBits = 14;  // cells per bucket: 2^14
+constexpr int kLocalBits = 13;           // cells per bucket: 2^13
 constexpr uint32_t kMaxBuckets = 16384;  // shared-memory cursors of the scatter (64 KB)
-constexpr uint64_t kHeavy = 1u << 18;   // particles above which a bucket takes the grid-wide path
-constexpr int BB_THREADS = 512;
-constexpr int BB_ITEMS = 8;             // particles per thread per iteration (six float4 loads)
+constexpr uint64_t kHeavy = 1u << 18;    // particles above which a bucket takes the grid-wide path
+constexpr int BB_THREADS = 512;          // histogram, scatter and heavy-scan blocks
+constexpr int BS_THREADS = 1024;         // bucket sort blocks (one per SM)
+constexpr uint32_t kStageCap = 11264;    // records of one bucket kept in shared memory (176 KB)
+constexpr int BB_ITEMS = 8;              // particles per thread per iteration (six float4 loads)
 constexpr uint64_t kChunkQuantum = 4096;
+
+struct alignas(32) PartRec {
+    uint32_t x, y, z, cell;
+    uint32_t pad[4];
+};
+static_assert(sizeof(PartRec) == 32, "partition records fill one 32-byte sector");
 
 struct BucketGeom {
     GridGeom g;
@@ -111,10 +130,20 @@ __global__ void __launch_bounds__(BB_THREADS) k_bucket_hist(const float* __restr
     for (uint32_t b = threadIdx.x; b < bg.nb; b += BB_THREADS) hist[(uint64_t)b * bg.C + blockIdx.x] = cnt[b];
 }
 
+// One 32-byte record (one 256-bit store: the sector is written whole).
+__device__ __forceinline__ void store_rec(PartRec* dst, float x, float y, float z, uint32_t cell) {
+    asm volatile("st.global.v8.b32 [%0], {%1, %2, %3, %4, %5, %5, %5, %5};" ::"l"(dst), "r"(__float_as_uint(x)),
+                 "r"(__float_as_uint(y)), "r"(__float_as_uint(z)), "r"(cell), "r"(0u)
+                 : "memory");
+}
+
+// The first 16 bytes of a record: (x, y, z, cell).
+__device__ __forceinline__ uint4 load_rec(const PartRec* src) { return __ldg(reinterpret_cast<const uint4*>(src)); }
+
 template <bool VEC>
 __global__ void __launch_bounds__(BB_THREADS) k_bucket_scatter(const float* __restrict__ xyz, BucketGeom bg,
                                                                const uint32_t* __restrict__ offs,
-                                                               uint4* __restrict__ part) {
+                                                               PartRec* __restrict__ part) {
     extern __shared__ uint32_t cur[];  // [nb]: next slot of each bucket for this chunk
     for (uint32_t b = threadIdx.x; b < bg.nb; b += BB_THREADS) cur[b] = offs[(uint64_t)b * bg.C + blockIdx.x];
     __syncthreads();
@@ -128,8 +157,7 @@ __global__ void __launch_bounds__(BB_THREADS) k_bucket_scatter(const float* __re
         for (int i = 0; i < BB_ITEMS; ++i) {
             if (valid & (1u << i)) {
                 const uint32_t slot = atomicAdd(&cur[key[i] >> bg.L], 1u);
-                part[slot] = make_uint4(__float_as_uint(f[3 * i]), __float_as_uint(f[3 * i + 1]),
-                                        __float_as_uint(f[3 * i + 2]), key[i]);
+                store_rec(part + slot, f[3 * i], f[3 * i + 1], f[3 * i + 2], key[i]);
             }
         }
     }
@@ -144,14 +172,14 @@ __device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v, int lane) {
     return v;
 }
 
-// In-place exclusive scan of a[0 .. 2^L) in shared memory by one block of
-// BB_THREADS threads: warp w scans its segment of 2^L / 16 entries (lanes
-// read consecutive words, no bank conflicts), then adds the totals of the
-// segments before it.
+// In-place exclusive scan of a[0 .. 2^L) in shared memory by the whole block
+// (a multiple of 32 threads, at most 1024): warp w scans its segment of
+// 2^L / warps entries (lanes read consecutive words, no bank conflicts), then
+// adds the totals of the segments before it.  wsum holds one word per warp.
 __device__ void block_excl_scan_cells(uint32_t* a, uint32_t ncells_pow2, uint32_t* wsum) {
-    constexpr int NW = BB_THREADS / 32;
+    const uint32_t NW = blockDim.x >> 5;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const uint32_t seg = ncells_pow2 / NW;  // >= 32 when 2^L >= 512, else handled by warp 0 alone
+    const uint32_t seg = ncells_pow2 / NW;  // >= 32 unless 2^L is small: then warp 0 alone
     if (seg >= 32) {
         uint32_t carry = 0;
         for (uint32_t k = 0; k < seg; k += 32) {
@@ -188,37 +216,48 @@ __device__ __forceinline__ void bucket_range(const BucketGeom& bg, const uint32_
     *be = (b + 1 < bg.nb) ? offs[(uint64_t)(b + 1) * bg.C] : (uint32_t)bg.n;
 }
 
-__global__ void __launch_bounds__(BB_THREADS) k_bucket_sort(const uint4* __restrict__ part, BucketGeom bg,
-                                                            const uint32_t* __restrict__ offs,
-                                                            float4* __restrict__ pts, uint32_t* __restrict__ cs,
-                                                            HeavyList hl) {
-    extern __shared__ uint32_t cnt[];  // [2^L]
-    __shared__ uint32_t wsum[BB_THREADS / 32];
-    const uint32_t b = blockIdx.x, tid = threadIdx.x;
+__global__ void __launch_bounds__(BS_THREADS, 1) k_bucket_sort(const PartRec* __restrict__ part, BucketGeom bg,
+                                                               const uint32_t* __restrict__ offs,
+                                                               float4* __restrict__ pts, uint32_t* __restrict__ cs,
+                                                               HeavyList hl) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    __shared__ uint32_t wsum[BS_THREADS / 32];
     const uint32_t ncl_pow2 = 1u << bg.L;
-    const uint64_t cell0 = (uint64_t)b << bg.L;
-    const uint32_t ncl = (uint32_t)min((uint64_t)ncl_pow2, bg.g.ncells - cell0);
-    uint32_t bs, be;
-    bucket_range(bg, offs, b, &bs, &be);
-    if (b == 0 && tid == 0) cs[bg.g.ncells] = (uint32_t)bg.n;
-    if ((uint64_t)(be - bs) > kHeavy) {
-        // the grid-wide kernels count this bucket in the cell table itself
-        for (uint32_t c = tid; c < ncl; c += BB_THREADS) cs[cell0 + c] = 0u;
-        if (tid == 0) hl.ids[atomicAdd(hl.count, 1u)] = b;
-        return;
-    }
-    for (uint32_t c = tid; c < ncl_pow2; c += BB_THREADS) cnt[c] = 0u;
-    __syncthreads();
+    uint32_t* cnt = smem;                                       // [2^L]
+    uint4* stage = reinterpret_cast<uint4*>(smem + ncl_pow2);   // [kStageCap]
+    const uint32_t tid = threadIdx.x, T = blockDim.x;
     const uint32_t mask = ncl_pow2 - 1u;
-    for (uint32_t i = bs + tid; i < be; i += BB_THREADS) atomicAdd(&cnt[part[i].w & mask], 1u);
-    __syncthreads();
-    block_excl_scan_cells(cnt, ncl_pow2, wsum);
-    for (uint32_t c = tid; c < ncl; c += BB_THREADS) cs[cell0 + c] = bs + cnt[c];
-    __syncthreads();
-    for (uint32_t i = bs + tid; i < be; i += BB_THREADS) {
-        const uint4 r = part[i];
-        const uint32_t slot = bs + atomicAdd(&cnt[r.w & mask], 1u);
-        pts[slot] = make_float4(__uint_as_float(r.x), __uint_as_float(r.y), __uint_as_float(r.z), 0.0f);
+    if (blockIdx.x == 0 && tid == 0) cs[bg.g.ncells] = (uint32_t)bg.n;
+    for (uint32_t b = blockIdx.x; b < bg.nb; b += gridDim.x) {
+        const uint64_t cell0 = (uint64_t)b << bg.L;
+        const uint32_t ncl = (uint32_t)min((uint64_t)ncl_pow2, bg.g.ncells - cell0);
+        uint32_t bs, be;
+        bucket_range(bg, offs, b, &bs, &be);
+        const uint32_t m = be - bs;
+        if ((uint64_t)m > kHeavy) {
+            // the grid-wide kernels count this bucket in the cell table itself
+            for (uint32_t c = tid; c < ncl; c += T) cs[cell0 + c] = 0u;
+            if (tid == 0) hl.ids[atomicAdd(hl.count, 1u)] = b;
+            continue;
+        }
+        const bool staged = m <= kStageCap;
+        for (uint32_t c = tid; c < ncl_pow2; c += T) cnt[c] = 0u;
+        __syncthreads();
+        for (uint32_t i = tid; i < m; i += T) {
+            const uint4 r = load_rec(part + bs + i);
+            if (staged) stage[i] = r;
+            atomicAdd(&cnt[r.w & mask], 1u);
+        }
+        __syncthreads();
+        block_excl_scan_cells(cnt, ncl_pow2, wsum);
+        for (uint32_t c = tid; c < ncl; c += T) cs[cell0 + c] = bs + cnt[c];
+        __syncthreads();
+        for (uint32_t i = tid; i < m; i += T) {
+            const uint4 r = staged ? stage[i] : load_rec(part + bs + i);
+            const uint32_t slot = bs + atomicAdd(&cnt[r.w & mask], 1u);
+            pts[slot] = make_float4(__uint_as_float(r.x), __uint_as_float(r.y), __uint_as_float(r.z), 0.0f);
+        }
+        __syncthreads();  // cnt and stage are reused by the next bucket
     }
 }
 
@@ -237,7 +276,7 @@ __device__ __forceinline__ uint32_t aggregated_add(uint32_t* ctr, uint32_t cell,
     return base + (uint32_t)__popc(peers & ((1u << lane) - 1u));
 }
 
-__global__ void k_heavy_count(const uint4* __restrict__ part, BucketGeom bg, const uint32_t* __restrict__ offs,
+__global__ void k_heavy_count(const PartRec* __restrict__ part, BucketGeom bg, const uint32_t* __restrict__ offs,
                               uint32_t* __restrict__ cs, HeavyList hl) {
     const uint32_t nh = *hl.count;
     const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
@@ -249,7 +288,7 @@ __global__ void k_heavy_count(const uint4* __restrict__ part, BucketGeom bg, con
         for (uint64_t base = bs + (t0 & ~31ull); base < be; base += T) {
             const uint64_t i = base + (t0 & 31);
             const bool live = i < be;
-            const uint32_t cell = live ? part[i].w : 0u;
+            const uint32_t cell = live ? load_rec(part + i).w : 0u;
             (void)aggregated_add(cs + cell, cell, live);
         }
     }
@@ -278,7 +317,7 @@ __global__ void __launch_bounds__(BB_THREADS) k_heavy_scan(BucketGeom bg, const 
     }
 }
 
-__global__ void k_heavy_scatter(const uint4* __restrict__ part, BucketGeom bg, const uint32_t* __restrict__ offs,
+__global__ void k_heavy_scatter(const PartRec* __restrict__ part, BucketGeom bg, const uint32_t* __restrict__ offs,
                                 float4* __restrict__ pts, HeavyList hl) {
     const uint32_t nh = *hl.count;
     const uint64_t T = (uint64_t)gridDim.x * blockDim.x;
@@ -291,7 +330,7 @@ __global__ void k_heavy_scatter(const uint4* __restrict__ part, BucketGeom bg, c
         for (uint64_t base = bs + (t0 & ~31ull); base < be; base += T) {
             const uint64_t i = base + (t0 & 31);
             const bool live = i < be;
-            const uint4 r = live ? part[i] : make_uint4(0u, 0u, 0u, 0u);
+            const uint4 r = live ? load_rec(part + i) : make_uint4(0u, 0u, 0u, 0u);
             const uint32_t local = r.w & mask;
             const uint32_t slot = aggregated_add(cur + local, local, live);
             if (live) pts[slot] = make_float4(__uint_as_float(r.x), __uint_as_float(r.y), __uint_as_float(r.z), 0.0f);
@@ -336,10 +375,15 @@ BucketBuildSizes bucket_build_sizes(const GridGeom& g, uint64_t n, int num_sms) 
     return z;
 }
 
+size_t bucket_record_bytes() { return sizeof(PartRec); }
+
 int build_grid_bucketed(const float* d_xyz, uint64_t n, const GridGeom& g, int num_sms, const BucketBuildBuffers& b,
                         cudaStream_t s) {
     const BucketGeom bg = bucket_geom(g, n, num_sms);
     const bool vec = (reinterpret_cast<uintptr_t>(d_xyz) & 15u) == 0;  // S * 12 bytes keeps chunks 16-byte aligned
+    if ((reinterpret_cast<uintptr_t>(b.part) & 31u) != 0)
+        return fail(SJCS_ERR_INVALID, "bucket build: the record buffer must be 32-byte aligned");
+    PartRec* part = static_cast<PartRec*>(b.part);
     const size_t smem_b = (size_t)bg.nb * sizeof(uint32_t);
     if (vec) {
         SJCS_CUDA_TRY(cudaFuncSetAttribute(k_bucket_hist<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
@@ -353,27 +397,29 @@ int build_grid_bucketed(const float* d_xyz, uint64_t n, const GridGeom& g, int n
     if (rc) return rc;
     if (vec) {
         SJCS_CUDA_TRY(cudaFuncSetAttribute(k_bucket_scatter<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
-        k_bucket_scatter<true><<<bg.C, BB_THREADS, smem_b, s>>>(d_xyz, bg, b.hist, b.part);
+        k_bucket_scatter<true><<<bg.C, BB_THREADS, smem_b, s>>>(d_xyz, bg, b.hist, part);
     } else {
         SJCS_CUDA_TRY(cudaFuncSetAttribute(k_bucket_scatter<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_b));
-        k_bucket_scatter<false><<<bg.C, BB_THREADS, smem_b, s>>>(d_xyz, bg, b.hist, b.part);
+        k_bucket_scatter<false><<<bg.C, BB_THREADS, smem_b, s>>>(d_xyz, bg, b.hist, part);
     }
     SJCS_LAUNCH_CHECK();
     k_zero_u32<<<1, 1, 0, s>>>(b.heavy_count);
     SJCS_LAUNCH_CHECK();
     const HeavyList hl{b.heavy_count, b.heavy_ids, b.cursors};
     const size_t smem_c = ((size_t)1 << bg.L) * sizeof(uint32_t);
-    SJCS_CUDA_TRY(cudaFuncSetAttribute(k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c));
-    k_bucket_sort<<<bg.nb, BB_THREADS, smem_c, s>>>(b.part, bg, b.hist, b.pts, b.cell_start, hl);
+    const size_t smem_s = smem_c + (size_t)kStageCap * sizeof(uint4);
+    SJCS_CUDA_TRY(cudaFuncSetAttribute(k_bucket_sort, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_s));
+    const unsigned sort_grid = std::min<unsigned>(bg.nb, (unsigned)num_sms);
+    k_bucket_sort<<<sort_grid, BS_THREADS, smem_s, s>>>(part, bg, b.hist, b.pts, b.cell_start, hl);
     SJCS_LAUNCH_CHECK();
     // buckets of more than kHeavy particles (none on uniform data): the three
     // kernels below find an empty list and return at once
-    k_heavy_count<<<num_sms * 4, 256, 0, s>>>(b.part, bg, b.hist, b.cell_start, hl);
+    k_heavy_count<<<num_sms * 4, 256, 0, s>>>(part, bg, b.hist, b.cell_start, hl);
     SJCS_LAUNCH_CHECK();
     SJCS_CUDA_TRY(cudaFuncSetAttribute(k_heavy_scan, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_c));
     k_heavy_scan<<<num_sms, BB_THREADS, smem_c, s>>>(bg, b.hist, b.cell_start, hl);
     SJCS_LAUNCH_CHECK();
-    k_heavy_scatter<<<num_sms * 4, 256, 0, s>>>(b.part, bg, b.hist, b.pts, hl);
+    k_heavy_scatter<<<num_sms * 4, 256, 0, s>>>(part, bg, b.hist, b.pts, hl);
     SJCS_LAUNCH_CHECK();
     return SJCS_OK;
 }

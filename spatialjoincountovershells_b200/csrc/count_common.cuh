@@ -32,8 +32,6 @@ struct CountParams {
     int periodic;
     int prune;
     uint32_t* __restrict__ counts;
-    uint32_t* err;                   // wait-error flag (host-mapped); null: no staged kernel
-    uint32_t stage_extra_bytes;      // 0 (a test hook adds bytes no copy delivers)
 };
 
 __device__ __forceinline__ float edge_margin(float v) { return 1e-3f + 2e-6f * fabsf(v); }
@@ -97,13 +95,6 @@ __device__ __forceinline__ Image make_image(const CountParams& p, float cx, floa
     return im;
 }
 
-__device__ __forceinline__ uint32_t lanes_below() {
-    uint32_t m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
-}
-
-// Called by all 32 lanes of the warp together (the candidate loops are warp-uniform).
 template <int BIN, bool BIG>
 __device__ __forceinline__ void test_candidate(const CountParams& p, const Image& im, const float4 pp, bool live,
                                                uint32_t* __restrict__ sink, const float* __restrict__ tab,
@@ -113,13 +104,7 @@ __device__ __forceinline__ void test_candidate(const CountParams& p, const Image
     const float dx = __fsub_rn(pp.x, im.cx), dy = __fsub_rn(pp.y, im.cy), dz = __fsub_rn(pp.z, im.cz);
     const float dist = __fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz));
     if (BIN != BIN_FIRST_MATCH) {
-        // Lanes that land in the same shell add once, with their number: most
-        // accepted candidates fall in the outermost shells (shell volume grows
-        // with r^3), and same-address atomics of one warp are serialised.
-        const bool acc = live && inb && dist < p.r2max;
-        const int b = acc ? bin_of<BIN>(p, tab, lut, dist) : -1;
-        const uint32_t peers = __match_any_sync(0xffffffffu, b);
-        if (acc && (peers & lanes_below()) == 0u) atomicAdd(sink + b, (uint32_t)__popc(peers));
+        if (live && inb && dist < p.r2max) atomicAdd(sink + bin_of<BIN>(p, tab, lut, dist), 1u);
     } else if (live && inb) {
         for (int i = 0; i < p.nrads; ++i) {
             if (dist < tab[i]) {

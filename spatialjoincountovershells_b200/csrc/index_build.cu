@@ -1,5 +1,5 @@
 // Plain (grid) index build for one particle file: the radix build below,
-// used for grids of more than 2^28 cells and by the allocation-free entry
+// used for grids of more than 2^27 cells and by the allocation-free entry
 // point; every other grid index is built by the two-pass bucket build
 // (bucket_build.cu).
 //
@@ -216,7 +216,7 @@ int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGe
         bb.pts = idx->pts;
         bb.cell_start = idx->cell_start;
         StreamScratch scr(s);  // freed (stream-ordered) on every return path
-        SJCS_CUDA_TRY(scr.alloc(&bb.part, z.part * sizeof(uint4)));
+        SJCS_CUDA_TRY(scr.alloc(&bb.part, z.part * bucket_record_bytes()));
         SJCS_CUDA_TRY(scr.alloc(&bb.hist, z.hist * sizeof(uint32_t)));
         SJCS_CUDA_TRY(scr.alloc(&bb.partials, z.partials * sizeof(uint32_t)));
         SJCS_CUDA_TRY(scr.alloc(&bb.heavy_count, sizeof(uint32_t)));

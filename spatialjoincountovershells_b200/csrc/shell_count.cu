@@ -324,175 +324,6 @@ __device__ __forceinline__ void count_batch(const CountParams& p, WarpPlans* wp,
     __syncwarp();  // the batch's plans are read before the next batch overwrites them
 }
 
-// ---- staged static schedule --------------------------------------------------
-//
-// The same batches and plans as count_batch, but the candidates of a halo's
-// planned rows reach the warp through shared memory: one lane per row issues
-// a bulk asynchronous copy (cp.async.bulk, completion counted in bytes on an
-// mbarrier) of the row's slot range to consecutive places of a per-warp
-// buffer, so the halo's candidates are one contiguous array -- lane l tests
-// candidates l, l+32, ... with no row lookup -- and the copies of halo k+1
-// run while halo k is tested.  Two buffers per warp alternate.  A halo with
-// more candidates than a buffer holds, with more than kMaxRows rows, or a
-// shifted periodic image, is counted from global memory as before.
-constexpr int kStageCap = 160;  // candidates per buffer (uniform R = 5 workloads: ~116 per halo)
-
-struct StageBuf {
-    float4 cand[2][kStageCap];
-    unsigned long long bar[2];
-};
-
-__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void bar_init(unsigned long long* bar) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
-}
-__device__ __forceinline__ void bar_arrive_expect(unsigned long long* bar, uint32_t bytes) {
-    asm volatile("{\n\t.reg .b64 st;\n\tmbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}" ::"r"(
-                     smem_addr(bar)),
-                 "r"(bytes)
-                 : "memory");
-}
-__device__ __forceinline__ bool bar_try_wait(unsigned long long* bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(smem_addr(bar)), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-// Bounded wait for the phase of `bar` with the given parity: false once about
-// 2^31 SM clocks (~1 s) have passed without it completing.
-__device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parity) {
-    if (bar_try_wait(bar, parity)) return true;
-    const long long t0 = clock64();
-    while (!bar_try_wait(bar, parity))
-        if (clock64() - t0 > (1ll << 31)) return false;
-    return true;
-}
-__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, unsigned long long* bar) {
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                     smem_addr(dst)),
-                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
-                 : "memory");
-}
-
-// Lane r < nrows holds row r's slot range [s0, s1).  Copies the rows, in
-// order, to buffer `buf` when they fit and returns their candidate count
-// (kStageCap + 1: they do not fit, nothing is copied).  Always arrives once
-// on the buffer's barrier (with the bytes to expect), so every issue is
-// matched by one wait.
-__device__ __forceinline__ uint32_t stage_rows(const CountParams& p, StageBuf* sb, int buf, uint32_t s0, uint32_t s1,
-                                               int lane) {
-    const uint32_t len = s1 - s0;
-    uint32_t incl = len;
-#pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-        const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
-        if (lane >= o) incl += v;
-    }
-    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
-    const bool fits = total <= (uint32_t)kStageCap;
-    // the buffer's previous contents were read by this warp's generic loads:
-    // order them before the asynchronous proxy writes it again
-    __syncwarp();
-    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-    if (fits && len) bulk_copy_g2s(&sb->cand[buf][incl - len], p.pts + s0, len * 16u, &sb->bar[buf]);
-    if (lane == 0) bar_arrive_expect(&sb->bar[buf], (fits ? total * 16u : 0u) + p.stage_extra_bytes);
-    return fits ? total : (uint32_t)kStageCap + 1u;
-}
-
-// Test the `total` staged candidates of buffer `buf` (two per lane per step).
-template <int BIN>
-__device__ __forceinline__ void run_staged(const CountParams& p, const Image& im, const float4* __restrict__ cand,
-                                           uint32_t total, uint32_t* __restrict__ sink, const float* __restrict__ tab,
-                                           const uint32_t* __restrict__ lut, int lane) {
-    for (uint32_t t0 = (uint32_t)lane; t0 < ((total + 63u) & ~63u); t0 += 64u) {
-        const uint32_t t1 = t0 + 32u;
-        const bool l0 = t0 < total, l1 = t1 < total;
-        const float4 p0 = l0 ? cand[t0] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 p1 = l1 ? cand[t1] : make_float4(0.f, 0.f, 0.f, 0.f);
-        test_candidate<BIN, false>(p, im, p0, l0, sink, tab, lut);
-        test_candidate<BIN, false>(p, im, p1, l1, sink, tab, lut);
-    }
-}
-
-// count_batch with staged candidates.  `ph` holds the two barriers' phase
-// parities (bit b: buffer b) and `live` turns false after a wait gave up
-// (the warp then stops counting; the host reports SJCS_ERR_TIMEOUT).
-template <int BIN>
-__device__ __forceinline__ void count_batch_staged(const CountParams& p, WarpPlans* wp, StageBuf* sb, uint32_t nb,
-                                                   float4 c_lane, uint32_t* __restrict__ wcnt,
-                                                   const float* __restrict__ tab, const uint32_t* __restrict__ lut,
-                                                   int lane, uint32_t* ph, bool* live) {
-    {
-        const bool valid = (uint32_t)lane < nb;
-        plan_halo(p, c_lane, valid, &wp->plan[lane], wp->row_cell[lane], wp->row_len[lane]);
-    }
-    __syncwarp();
-    auto rows_of = [&](uint32_t k) {
-        const uint32_t nr = wp->plan[k].nrows;
-        return nr == kSlowPlan ? 0u : nr;
-    };
-    // slot ranges: halo k (a0, b0), k+1 (a1, b1); staged count of halo k
-    uint32_t a0, b0, a1 = 0, b1 = 0;
-    fetch_rows(p, wp, 0, rows_of(0), lane, &a0, &b0);
-    uint32_t n0 = stage_rows(p, sb, 0, a0, b0, lane);
-    if (nb > 1) fetch_rows(p, wp, 1, rows_of(1), lane, &a1, &b1);
-    uint32_t n1 = 0;
-    for (uint32_t k = 0; k < nb; ++k) {
-        const int buf = (int)(k & 1u);
-        if (k + 1 < nb) n1 = stage_rows(p, sb, buf ^ 1, a1, b1, lane);
-        uint32_t a2 = 0, b2 = 0;
-        if (k + 2 < nb) fetch_rows(p, wp, k + 2, rows_of(k + 2), lane, &a2, &b2);
-        const HaloPlan pl = wp->plan[k];
-        const uint32_t parity = (*ph >> buf) & 1u;
-        if (!bar_wait(&sb->bar[buf], parity)) {
-            // flag the failure, give the copies in flight (this buffer's and
-            // the next halo's) one more bounded wait each, and stop counting
-            if (lane == 0) {
-                *reinterpret_cast<volatile uint32_t*>(p.err) = 1u;
-                __threadfence_system();
-            }
-            (void)bar_wait(&sb->bar[buf], parity);
-            if (k + 1 < nb) (void)bar_wait(&sb->bar[buf ^ 1], (*ph >> (buf ^ 1)) & 1u);
-            *live = false;
-            break;
-        }
-        *ph ^= 1u << buf;
-        {
-            uint32_t* row = p.counts + (uint64_t)pl.row * (uint64_t)p.nrads;
-            Image im;
-            im.cx = pl.cx;
-            im.cy = pl.cy;
-            im.cz = pl.cz;
-            im.lox = __fsub_rn(pl.cx, p.half);
-            im.hix = __fadd_rn(pl.cx, p.half);
-            im.loy = __fsub_rn(pl.cy, p.half);
-            im.hiy = __fadd_rn(pl.cy, p.half);
-            im.loz = __fsub_rn(pl.cz, p.half);
-            im.hiz = __fadd_rn(pl.cz, p.half);
-            if (pl.nrows == kSlowPlan) {
-                count_image<BIN, false>(p, make_image(p, pl.cx, pl.cy, pl.cz), 0, wcnt, tab, lut, lane);
-            } else if (n0 > (uint32_t)kStageCap) {
-                run_rows<BIN, false>(p, im, a0, b0, wcnt, tab, lut, lane);
-            } else {
-                run_staged<BIN>(p, im, sb->cand[buf], n0, wcnt, tab, lut, lane);
-            }
-            if (pl.flags)
-                count_shifted_images<BIN, false>(p, make_float4(pl.cx, pl.cy, pl.cz, 0.f), wcnt, tab, lut, lane);
-            flush_counts(p, wcnt, row, lane);
-        }
-        a0 = a1;
-        b0 = b1;
-        a1 = a2;
-        b1 = b2;
-        n0 = n1;
-    }
-    __syncwarp();  // the batch's plans are read before the next batch overwrites them
-}
-
 // Shared-memory set-up common to both schedules: per-warp plans, the r2
 // table, the shell lookup table and per-warp counters.
 struct SmemView {
@@ -535,32 +366,6 @@ __global__ void __launch_bounds__(CT_THREADS, 8) k_shell_count(CountParams p) {
         const uint32_t nb = (uint32_t)min((uint64_t)kBatch, mine - b0);
         const float4 c = (uint32_t)lane < nb ? p.halos[(b0 + lane) * W + gw] : make_float4(0.f, 0.f, 0.f, 0.f);
         count_batch<BIN, BIG>(p, v.wp, nb, c, v.wcnt, v.tab, v.lut, lane);
-    }
-}
-
-// Static schedule with staged candidates (the shared-memory table forms).
-template <int BIN>
-__global__ void __launch_bounds__(CT_THREADS, 4) k_shell_count_staged(CountParams p) {
-    extern __shared__ __align__(16) uint32_t smem[];
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    StageBuf* sb = reinterpret_cast<StageBuf*>(smem) + warp;
-    uint32_t* rest = reinterpret_cast<uint32_t*>(reinterpret_cast<StageBuf*>(smem) + CT_WARPS);
-    const SmemView v = setup_smem<false>(p, rest, tid, warp);
-    if (lane == 0) {
-        bar_init(&sb->bar[0]);
-        bar_init(&sb->bar[1]);
-        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-    }
-    __syncthreads();
-    const uint64_t W = (uint64_t)gridDim.x * CT_WARPS;
-    const uint64_t gw = (uint64_t)blockIdx.x * CT_WARPS + warp;
-    const uint64_t mine = p.nhalos > gw ? (p.nhalos - gw + W - 1) / W : 0;  // halos of this warp
-    uint32_t ph = 0;
-    bool live = true;
-    for (uint64_t b0 = 0; b0 < mine && live; b0 += kBatch) {
-        const uint32_t nb = (uint32_t)min((uint64_t)kBatch, mine - b0);
-        const float4 c = (uint32_t)lane < nb ? p.halos[(b0 + lane) * W + gw] : make_float4(0.f, 0.f, 0.f, 0.f);
-        count_batch_staged<BIN>(p, v.wp, sb, nb, c, v.wcnt, v.tab, v.lut, lane, &ph, &live);
     }
 }
 
@@ -678,22 +483,6 @@ int launch_variant(sjcs_ctx* ctx, const CountParams& p, size_t smem, cudaStream_
     return SJCS_OK;
 }
 
-template <int BIN>
-int launch_staged(sjcs_ctx* ctx, const CountParams& p, size_t smem, cudaStream_t s) {
-    auto kern = k_shell_count_staged<BIN>;
-    if (smem > 48 * 1024)
-        SJCS_CUDA_TRY(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm = 0;
-    SJCS_CUDA_TRY(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, CT_THREADS, smem));
-    if (per_sm < 1) per_sm = 1;
-    const uint64_t want = (p.nhalos + CT_WARPS - 1) / CT_WARPS;
-    const uint64_t cap = (uint64_t)ctx->num_sms * (uint64_t)per_sm;
-    const unsigned grid = (unsigned)(want < cap ? want : cap);
-    kern<<<grid, CT_THREADS, smem, s>>>(p);
-    SJCS_LAUNCH_CHECK();
-    return SJCS_OK;
-}
-
 template <int BIN, bool BIG>
 int launch_queue(sjcs_ctx* ctx, const CountParams& p, const Schedule& sc, size_t smem, cudaStream_t s) {
     const uint64_t n = p.nhalos;
@@ -751,8 +540,6 @@ int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx
     p.periodic = (q->flags & SJCS_QUERY_PERIODIC) ? 1 : 0;
     p.prune = q->monotone && std::isfinite(q->r2max) ? 1 : 0;
     p.counts = q->counts;
-    p.err = ctx->d_err;
-    p.stage_extra_bytes = ctx->stage_extra;
     const int bin = !q->monotone ? BIN_FIRST_MATCH : (q->nlut > 0 ? BIN_LUT : BIN_BSEARCH);
     const bool big = q->pad > kMaxSmemTable || q->nrads > kMaxSmemRads;
     if (big) p.nlut = q->nlut;  // table and LUT are read from global memory
@@ -770,12 +557,6 @@ int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx
                 return big ? launch_queue<BIN_FIRST_MATCH, true>(ctx, p, *sc, smem, s)
                            : launch_queue<BIN_FIRST_MATCH, false>(ctx, p, *sc, smem, s);
         }
-    }
-    // static schedule with the tables in shared memory: staged candidates
-    // (needs the context's wait-error flag)
-    if (!big && bin != BIN_FIRST_MATCH && p.err) {
-        const size_t smem_st = CT_WARPS * sizeof(StageBuf) + smem;
-        return bin == BIN_LUT ? launch_staged<BIN_LUT>(ctx, p, smem_st, s) : launch_staged<BIN_BSEARCH>(ctx, p, smem_st, s);
     }
     switch (bin) {
         case BIN_LUT:

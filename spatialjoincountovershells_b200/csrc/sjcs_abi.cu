@@ -68,24 +68,6 @@ __global__ void k_fill_f32(float* __restrict__ p, uint64_t m, float v) {
 }
 
 bool valid_ctx(const sjcs_ctx* c) { return c && c->magic == kCtxMagic; }
-
-}  // namespace
-
-// After waiting for a context's work: SJCS_ERR_TIMEOUT if one of its kernels
-// gave up a bounded wait (the flag is cleared; the counts of that launch are
-// incomplete).
-int wait_errors(sjcs_ctx* ctx) {
-    volatile uint32_t* f = ctx ? ctx->h_err : nullptr;
-    if (f && *f) {
-        *f = 0u;
-        return fail(SJCS_ERR_TIMEOUT,
-                    "a count kernel gave up waiting for its staged candidate copies; the counts of that launch "
-                    "are incomplete");
-    }
-    return SJCS_OK;
-}
-
-namespace {
 bool valid_index(const sjcs_index* i) { return i && i->magic == kIndexMagic; }
 bool valid_query(const sjcs_query* q) { return q && q->magic == kQueryMagic; }
 
@@ -549,11 +531,6 @@ int sjcs_ctx_create(int device, sjcs_ctx** out) {
     SJCS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->s_read, cudaStreamNonBlocking));
     SJCS_CUDA_TRY(cudaStreamCreateWithFlags(&ctx->s_h2d, cudaStreamNonBlocking));
     SJCS_CUDA_TRY(cudaEventCreateWithFlags(&ctx->ev_counts, cudaEventDisableTiming));
-    // Wait-error flag: page-locked host memory the kernels write through its
-    // device mapping when a bounded wait gives up; read after each wait.
-    SJCS_CUDA_TRY(cudaHostAlloc(reinterpret_cast<void**>(&ctx->h_err), sizeof(uint32_t), cudaHostAllocMapped));
-    *ctx->h_err = 0u;
-    SJCS_CUDA_TRY(cudaHostGetDevicePointer(reinterpret_cast<void**>(&ctx->d_err), ctx->h_err, 0));
     // Keep freed stream-ordered memory cached in the pool: every file's index
     // and scratch reuse the previous file's pages without new cudaMalloc calls.
     cudaMemPool_t pool;
@@ -581,16 +558,8 @@ int sjcs_ctx_destroy(sjcs_ctx* ctx) {
         if (e) cudaEventDestroy(e);
     if (ctx->ring) cudaFreeHost(ctx->ring);
     if (ctx->ev_counts) cudaEventDestroy(ctx->ev_counts);
-    if (ctx->h_err) cudaFreeHost(ctx->h_err);
     ctx->magic = 0;
     delete ctx;
-    return SJCS_OK;
-}
-
-int sjcs_ctx_set_wait_test(sjcs_ctx* ctx, uint32_t extra_bytes) {
-    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
-    std::lock_guard<std::mutex> lk(ctx->mu);
-    ctx->stage_extra = extra_bytes;
     return SJCS_OK;
 }
 
@@ -602,7 +571,7 @@ int sjcs_ctx_sync(sjcs_ctx* ctx) {
     SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_count));
     SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_read));
     SJCS_CUDA_TRY(cudaStreamSynchronize(ctx->s_h2d));
-    return wait_errors(ctx);
+    return SJCS_OK;
 }
 
 int sjcs_ctx_stream(const sjcs_ctx* ctx, int which, void** stream) {
@@ -1188,7 +1157,7 @@ int sjcs_step_launch(sjcs_ctx* ctx, sjcs_step* st) {
 int sjcs_step_wait(sjcs_step* st) {
     if (!valid_step(st)) return fail(SJCS_ERR_STATE, "invalid step");
     if (st->launched) SJCS_CUDA_TRY(cudaEventSynchronize(st->ev1));
-    return wait_errors(st->ctx);
+    return SJCS_OK;
 }
 
 int sjcs_step_time(sjcs_step* st, float* ms) {
@@ -1302,7 +1271,7 @@ int sjcs_autotune(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx, sjcs_sche
 int sjcs_query_wait(sjcs_query* q) {
     if (!valid_query(q)) return fail(SJCS_ERR_STATE, "invalid query");
     SJCS_CUDA_TRY(cudaEventSynchronize(q->ev_last));
-    return wait_errors(q->ctx);
+    return SJCS_OK;
 }
 
 int sjcs_query_read_counts(sjcs_ctx* ctx, sjcs_query* q, uint64_t* counts, int accumulate) {
@@ -1363,7 +1332,7 @@ int sjcs_query_read_counts(sjcs_ctx* ctx, sjcs_query* q, uint64_t* counts, int a
     float ms = 0.f;
     q->last_d2h_ms = (cudaEventElapsedTime(&ms, q->ev_d0, q->ev_d1) == cudaSuccess) ? ms : 0.f;
     cudaGetLastError();
-    return wait_errors(ctx);
+    return SJCS_OK;
 }
 
 int sjcs_query_read_counts_async(sjcs_ctx* ctx, sjcs_query* q, uint64_t* counts) {
@@ -1400,7 +1369,7 @@ int sjcs_query_wait_read(sjcs_query* q) {
     float ms = 0.f;
     q->last_d2h_ms = (cudaEventElapsedTime(&ms, q->ev_d0, q->ev_d1) == cudaSuccess) ? ms : 0.f;
     cudaGetLastError();
-    return wait_errors(q->ctx);
+    return SJCS_OK;
 }
 
 int sjcs_query_device_counts(const sjcs_query* q, uint32_t** d_counts) {

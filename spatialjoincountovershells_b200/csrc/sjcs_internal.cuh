@@ -131,11 +131,6 @@ struct sjcs_ctx {
     std::mutex ring_mu;
     char* ring = nullptr;
     std::vector<cudaEvent_t> ring_ev;
-    // Set (to 1) by a kernel whose bounded wait gave up; page-locked and
-    // mapped, so the host reads it after a wait without a copy.
-    uint32_t* h_err = nullptr;
-    uint32_t* d_err = nullptr;  // device address of *h_err
-    uint32_t stage_extra = 0;   // test hook: bytes the count kernel's staged copies over-expect
 };
 
 namespace sjcs {
@@ -217,10 +212,6 @@ constexpr uint32_t kCtxMagic = 0x534a4358u;    // "SJCX"
 constexpr uint32_t kIndexMagic = 0x534a4958u;  // "SJIX"
 constexpr uint32_t kQueryMagic = 0x534a5158u;  // "SJQX"
 
-// sjcs_abi.cu: SJCS_ERR_TIMEOUT (and the flag cleared) if one of ctx's
-// kernels gave up a bounded wait since the last check, else SJCS_OK.
-int wait_errors(sjcs_ctx* ctx);
-
 // index_build.cu
 int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGeom& g,
                      sjcs_index* idx, cudaStream_t s);
@@ -296,12 +287,12 @@ int grid_key_bits(const GridGeom& g);
 int grid_digit_bits(const GridGeom& g);  // 9 for 25-27-bit cell keys, else 8
 int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, cudaStream_t s);
 // bucket_build.cu: the grid build in two passes over the particles --
-// partition into buckets of 2^14 consecutive cells, then a counting sort of
+// partition into buckets of 2^13 consecutive cells, then a counting sort of
 // each bucket that also writes its cells' cell_start entries.  Grids whose
 // buckets would not fit the partition's shared-memory cursors (more than
-// 2^28 cells) use the radix build above.  Sizes are element counts.
+// 2^27 cells) use the radix build above.  Sizes are element counts.
 struct BucketBuildSizes {
-    uint64_t part;       // uint4 records (x, y, z, cell)
+    uint64_t part;       // records of bucket_record_bytes() (x, y, z, cell, padding)
     uint64_t hist;       // u32 per (bucket, chunk)
     uint64_t partials;   // u32 scan partials of hist
     uint64_t max_heavy;  // u32 ids of buckets of more than 2^18 particles
@@ -310,13 +301,14 @@ struct BucketBuildSizes {
 struct BucketBuildBuffers {
     float4* pts;           // n sorted particles (output)
     uint32_t* cell_start;  // ncells + 1 (output)
-    uint4* part;
+    void* part;             // 32-byte aligned
     uint32_t* hist;
     uint32_t* partials;
     uint32_t* heavy_count;  // 1
     uint32_t* heavy_ids;
     uint32_t* cursors;
 };
+size_t bucket_record_bytes();
 bool bucket_build_eligible(const GridGeom& g, uint64_t n);
 BucketBuildSizes bucket_build_sizes(const GridGeom& g, uint64_t n, int num_sms);
 int build_grid_bucketed(const float* d_xyz, uint64_t n, const GridGeom& g, int num_sms, const BucketBuildBuffers& b,

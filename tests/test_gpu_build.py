@@ -86,7 +86,7 @@ def test_bucket_build_at_the_automatic_2_27_cell_grid(ctx):
     p = nat.gen_uniform_particles(1, 1, n)
     dp = torch.from_numpy(p).cuda()
     idx = ctx.build_index(dp, radius_hint=5.0)
-    assert idx.grid() == (942, 377, 377)
+    assert idx.grid == (942, 377, 377)
     rng = np.random.default_rng(66)
     h = nat.gen_uniform_halos(2, 20000)["point"].copy()
     h[:600] = rng.choice([0.0, 999.999, 1.5, 998.5, 4.99, 995.01], size=(600, 3))
