@@ -434,6 +434,16 @@ def run_ours(args, w, dist, rank, world, local):
     grid_counts = device_counts(q)
     sample = {"grid": grid_counts[:nhs * nr].cpu().numpy().view(np.uint32).reshape(nhs, nr)}
     q.destroy()
+    # the build kernels alone (no count queued before them), for the build roofline
+    bk, ncells = [], None
+    for _ in range(2):
+        for f in range(nf):
+            idx = ctx.build_index(parts_d[f], radius_hint=R)
+            idx.wait()
+            bk.append(idx.timing()["build_ms"])
+            g = idx.grid
+            ncells = g[0] * g[1] * g[2]
+            idx.destroy()
 
     def counts_of(kind, mode):
         qq = ctx.query(halos_d, r2)
@@ -505,6 +515,13 @@ def run_ours(args, w, dist, rank, world, local):
                 "kernel": "k_shell_count", "launch_ms": round(count_ms, 3),
                 "algorithmic_bytes_per_launch": ALGO_BYTES_PER_HALO_FILE * nh,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
+    build_ms = statistics.median(bk)
+    build_bytes = 24.0 * n + 4.0 * (ncells + 1)  # 12 B read + 12 B written per particle, 4 B per cell
+    roof_build = {"bound": "hbm", "achieved": round(build_bytes / (build_ms / 1e3) / 1e9, 1), "peak": peak,
+                  "unit": "GB/s", "frac": round(build_bytes / (build_ms / 1e3) / 1e9 / peak, 4),
+                  "kernel": "grid index build (k_bucket_hist + scan + k_bucket_scatter + k_bucket_sort)",
+                  "build_ms": round(build_ms, 3), "algorithmic_bytes_per_build": build_bytes,
+                  "cells": int(ncells)}
 
     # the reference program on the same host: every particle file of the
     # step and the first nhs halos; its result text is the parity check of
@@ -534,6 +551,7 @@ def run_ours(args, w, dist, rank, world, local):
             "d2h_bytes_per_step": int(nh * nr * 8),
             "pipeline": "job k's read-back overlaps job k+1's uploads (2 jobs in flight)"},
         "roofline": roof,
+        "roofline_build": roof_build,
         "cpu_baseline": cpu,
         "clocks": clocks,
         "clocks_e2e": clocks_e2e,

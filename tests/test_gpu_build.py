@@ -1,7 +1,8 @@
-"""Grid index builds on the GPU: the two-pass bucket build, its grid-wide path
-for buckets of more than 2^18 particles, and the radix build kept for grids of
-more than 2^28 cells.  Whatever path builds the index, the counts must equal
-the oracle's (which is pinned to the reference's own outputs)."""
+"""Grid index builds on the GPU: the two-pass bucket build (partition into
+buckets of 2^16 cells, then a counting sort of each bucket by a cluster of 8
+blocks), on dense clumps, a single crowded cell, odd and very large grids.
+The counts must equal the oracle's (which is pinned to the reference's own
+outputs)."""
 from __future__ import annotations
 
 import numpy as np
@@ -29,9 +30,9 @@ def _halos_around(rng, centre, spread, n_near, n_far):
     return np.concatenate([near, far, [[0, 0, 0], [999.99, 0.5, 500]]]).astype(np.float32) % np.float32(1000)
 
 
-def test_heavy_buckets_take_the_grid_wide_path(ctx):
+def test_dense_buckets(ctx):
     """600k particles, 80 % in a ball of radius 1: the buckets around the ball
-    hold far more than 2^18 particles each."""
+    hold far more records than the sort blocks keep in shared memory."""
     rng = np.random.default_rng(61)
     n = 600_000
     p = rng.uniform(0, 1000, size=(n, 3))
@@ -65,10 +66,11 @@ def test_clustered_file_matches_oracle(ctx):
     assert np.array_equal(_counts(ctx, p, h, r2, hint=20.0), oracle.count(p, h, r2))
 
 
-@pytest.mark.parametrize("grid", [(2048, 512, 512), (1, 1, 1), (3, 1, 70001 // 3)])
-def test_radix_build_and_tiny_or_odd_grids(grid, ctx):
-    """More than 2^28 cells: the radix build; one cell; cell counts that are
-    not a multiple of the bucket size."""
+@pytest.mark.parametrize("grid", [(2048, 512, 512), (4096, 512, 600), (1, 1, 1), (3, 1, 70001 // 3), (5, 1, 1)])
+def test_large_tiny_and_odd_grids(grid, ctx):
+    """2^29 cells (8192 buckets); more than 2^30 cells (the radix build); one
+    cell; cell counts that are not a multiple of the bucket size; buckets of
+    fewer cells than a cluster has blocks."""
     rng = np.random.default_rng(65)
     p = rng.uniform(0, 1000, size=(120_000, 3)).astype(np.float32)
     h = rng.uniform(0, 1000, size=(1500, 3)).astype(np.float32)
@@ -77,16 +79,16 @@ def test_radix_build_and_tiny_or_odd_grids(grid, ctx):
     assert np.array_equal(_counts(ctx, p, h, r2, grid=grid, hint=12.0), oracle.count(p, h, r2))
 
 
-def test_bucket_build_at_the_automatic_2_27_cell_grid(ctx):
-    """1e8 uniform particles (the README-scale file): 942 x 377 x 377 cells,
-    27-bit cell ids, 8172 buckets; 20000 halos including face and corner
-    halos checked against the oracle."""
+def test_bucket_build_at_the_automatic_readme_scale_grid(ctx):
+    """1e8 uniform particles (the README-scale file): 1000 x 400 x 400 cells,
+    28-bit cell ids, 2442 buckets sorted by clusters of 8 blocks; 20000 halos
+    including face and corner halos checked against the oracle."""
     import torch
     n = 100_000_000
     p = nat.gen_uniform_particles(1, 1, n)
     dp = torch.from_numpy(p).cuda()
     idx = ctx.build_index(dp, radius_hint=5.0)
-    assert idx.grid == (942, 377, 377)
+    assert idx.grid == (1000, 400, 400)
     rng = np.random.default_rng(66)
     h = nat.gen_uniform_halos(2, 20000)["point"].copy()
     h[:600] = rng.choice([0.0, 999.999, 1.5, 998.5, 4.99, 995.01], size=(600, 3))
