@@ -519,7 +519,7 @@ def run_ours(args, w, dist, rank, world, local):
     build_bytes = 24.0 * n + 4.0 * (ncells + 1)  # 12 B read + 12 B written per particle, 4 B per cell
     roof_build = {"bound": "hbm", "achieved": round(build_bytes / (build_ms / 1e3) / 1e9, 1), "peak": peak,
                   "unit": "GB/s", "frac": round(build_bytes / (build_ms / 1e3) / 1e9 / peak, 4),
-                  "kernel": "grid index build (k_bucket_hist + scan + k_bucket_scatter + k_bucket_sort)",
+                  "kernel": "grid index build (radix passes k_radix_upsweep* + scan + k_radix_downsweep, k_cell_start)",
                   "build_ms": round(build_ms, 3), "algorithmic_bytes_per_build": build_bytes,
                   "cells": int(ncells)}
 

@@ -197,7 +197,12 @@ int sjcs_host_free(void *p);
  * refuses to build it, src/objects/ArraySTR/Build.c:860-863). */
 int sjcs_index_build(sjcs_ctx *ctx, const float *xyz, uint64_t n,
                      const sjcs_index_opts *opts, sjcs_index **out);
-/* Same, with the particles already in device memory (d_xyz, n*3 floats). */
+/* Same, with the particles already in device memory (d_xyz, n*3 floats).
+ * The build runs on the context's build stream (sjcs_ctx_stream, which = 0):
+ * work that writes d_xyz on another stream must be ordered before it by the
+ * caller (e.g. cudaEventRecord on the producer's stream and
+ * cudaStreamWaitEvent on the build stream), and d_xyz must stay untouched
+ * until sjcs_index_wait.  The Python binding does both for CUDA tensors. */
 int sjcs_index_build_device(sjcs_ctx *ctx, const float *d_xyz, uint64_t n,
                             const sjcs_index_opts *opts, sjcs_index **out);
 /* Same, reading a decoded particle file (x,y,z float triplets, count =
@@ -261,7 +266,9 @@ int sjcs_index_destroy(sjcs_index *idx);
 int sjcs_query_create(sjcs_ctx *ctx, const float *halo_xyz, size_t stride_bytes,
                       uint64_t nhalos, const float *r2, int nrads, int flags,
                       sjcs_query **out);
-/* Same, halos already in device memory. */
+/* Same, halos already in device memory; the halo upload runs on the count
+ * stream (sjcs_ctx_stream, which = 1), which the caller orders after the
+ * halos' producer. */
 int sjcs_query_create_device(sjcs_ctx *ctx, const float *d_halo_xyz, size_t stride_bytes,
                              uint64_t nhalos, const float *r2, int nrads, int flags,
                              sjcs_query **out);

@@ -226,6 +226,17 @@ def _is_cuda(a) -> bool:
     return hasattr(a, "is_cuda") and bool(a.is_cuda)
 
 
+def _hand_over(ctx: "Context", which: int, t) -> None:
+    """Order the library's stream `which` (0 build, 1 count) after the work
+    queued on torch's current stream (the producer of tensor t), and keep t's
+    memory out of torch's allocator until the library's work queued on that
+    stream so far has finished."""
+    import torch
+    s = torch.cuda.ExternalStream(ctx.stream(which), device=t.device)
+    s.wait_stream(torch.cuda.current_stream(t.device))
+    t.record_stream(s)
+
+
 def _as_f32_xyz(a) -> np.ndarray:
     a = np.ascontiguousarray(a, dtype=np.float32)
     if a.ndim != 2 or a.shape[1] != 3:
@@ -298,6 +309,7 @@ class Context:
         h = _vp()
         if _is_cuda(xyz):
             n = xyz.numel() // 3
+            _hand_over(self, 0, xyz)
             _check(lib().sjcs_index_build_device(self._h, _vp(xyz.data_ptr()), n, _c.byref(opts), _c.byref(h)))
             keep = xyz
         else:
@@ -370,6 +382,7 @@ class Context:
         if _is_cuda(halos):
             stride = 4 * (halos.shape[-1] if halos.dim() == 2 else 3)
             n = halos.shape[0] if halos.dim() == 2 else halos.numel() // 3
+            _hand_over(self, 1, halos)
             _check(lib().sjcs_query_create_device(self._h, _vp(halos.data_ptr()), stride, n,
                                                   _vp(r2.ctypes.data), len(r2), flags, _c.byref(h)))
             keep = halos

@@ -25,7 +25,7 @@ INCLUDE = ROOT / "include"
 
 CUDA_SOURCES = [
     "sjcs_abi.cu", "index_build.cu", "learned_index.cu", "query_prep.cu", "shell_count.cu", "morton_count.cu",
-    "scan.cu", "serve.cu", "decode.cu", "noalloc.cu", "bucket_build.cu",
+    "scan.cu", "serve.cu", "decode.cu", "noalloc.cu",
 ]
 HOST_SOURCES = ["sjcs_io.c", "sjcs_gen.c"]
 

@@ -1,7 +1,4 @@
-// Plain (grid) index build for one particle file: the radix build below,
-// used for grids of more than 2^30 cells and by the allocation-free entry
-// point; every other grid index is built by the two-pass bucket build
-// (bucket_build.cu).
+// Plain (grid) index build for one particle file.
 //
 // Replaces the STR bulk load of the reference (MakeTreeWithSameThreadPoolArraySTR,
 // src/objects/ArraySTR/Build.c:845-963: per level, LSD radix sorts on the
@@ -126,11 +123,11 @@ GridGeom auto_grid(uint64_t n, float radius_hint, const uint32_t* grid_req) {
     } else {
         // Rows of cells run along x and are looked up with two offsets, so x
         // can be finer than y/z for free: cells are 2.5x longer in y and z.
-        // Target about 1.6 cells per particle, at most 2^28 cells (1 GB of
-        // cell table), and keep y/z cells >= R/4: a query box then spans at
-        // most 9x9 rows (boxes of more than 25 rows are counted without the
-        // per-batch row plan).
-        constexpr double kMaxCells = 268435456.0;  // 2^28
+        // Target about 1.6 cells per particle, at most 2^27 cells (a 27-bit
+        // cell key sorts in three 9-bit radix passes), and keep y/z cells
+        // >= R/4: a query box then spans at most 9x9 rows (boxes of more
+        // than 25 rows are counted without the per-batch row plan).
+        constexpr double kMaxCells = 134217728.0;  // 2^27
         const double target = std::min(std::max(1.6 * (double)n, 4096.0), kMaxCells);
         double hyz = std::cbrt(2.5e9 / target);
         if (radius_hint > 0.0f) hyz = std::max(hyz, 0.25 * (double)radius_hint);
@@ -202,25 +199,11 @@ int fill_cell_table(const uint32_t* sorted_cells, uint64_t n, uint64_t ncells, u
 
 int build_grid_index(sjcs_ctx* ctx, const float* d_xyz, uint64_t n, const GridGeom& g,
                      sjcs_index* idx, cudaStream_t s) {
+    (void)ctx;
     idx->geom = g;
     const uint64_t nalloc = n ? n : 1;
     SJCS_CUDA_TRY(cudaMallocAsync(&idx->pts, nalloc * sizeof(float4), s));
     SJCS_CUDA_TRY(cudaMallocAsync(&idx->cell_start, (g.ncells + 1) * sizeof(uint32_t), s));
-    if (n == 0) {
-        SJCS_CUDA_TRY(cudaMemsetAsync(idx->cell_start, 0, (g.ncells + 1) * sizeof(uint32_t), s));
-        return SJCS_OK;
-    }
-    if (bucket_build_eligible(g, n)) {
-        const BucketBuildSizes z = bucket_build_sizes(g, n, ctx->num_sms);
-        BucketBuildBuffers bb{};
-        bb.pts = idx->pts;
-        bb.cell_start = idx->cell_start;
-        StreamScratch scr(s);  // freed (stream-ordered) on every return path
-        SJCS_CUDA_TRY(scr.alloc(&bb.part, z.part * sizeof(uint4)));
-        SJCS_CUDA_TRY(scr.alloc(&bb.hist, z.hist * sizeof(uint32_t)));
-        SJCS_CUDA_TRY(scr.alloc(&bb.partials, z.partials * sizeof(uint32_t)));
-        return build_grid_bucketed(d_xyz, n, g, ctx->num_sms, bb, s);
-    }
 
     GridBuildBuffers b{};
     b.pts = idx->pts;

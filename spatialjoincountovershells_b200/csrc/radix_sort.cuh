@@ -321,7 +321,9 @@ k_radix_downsweep(KeyOp kop, PayOp pop, uint64_t n, int shift,
             } else {
                 v = kAsync ? xpay[xsrc[j]] : xpay[j];
             }
-            sink(gbase[d] + (j - dstart[d]), kk, v);
+            // in bounds unless the input changed between the histogram and this pass
+            const uint32_t gpos = gbase[d] + (j - dstart[d]);
+            if (gpos < n) sink(gpos, kk, v);
         }
     }
 }

@@ -286,28 +286,6 @@ constexpr uint32_t kGridGaps = 1u << 16;
 int grid_key_bits(const GridGeom& g);
 int grid_digit_bits(const GridGeom& g);  // 9 for 25-27-bit cell keys, else 8
 int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, cudaStream_t s);
-// bucket_build.cu: the grid build in two passes over the particles --
-// partition into buckets of 2^16 consecutive cells, then a counting sort of
-// each bucket by a cluster of 8 blocks that also writes its cells'
-// cell_start entries.  Grids whose buckets would not fit the partition's
-// shared-memory cursors (more than 2^30 cells) use the radix build above.
-// Sizes are element counts.
-struct BucketBuildSizes {
-    uint64_t part;       // uint4 records (x, y, z, cell)
-    uint64_t hist;       // u32 per (bucket, chunk)
-    uint64_t partials;   // u32 scan partials of hist
-};
-struct BucketBuildBuffers {
-    float4* pts;           // n sorted particles (output)
-    uint32_t* cell_start;  // ncells + 1 (output)
-    uint4* part;
-    uint32_t* hist;
-    uint32_t* partials;
-};
-bool bucket_build_eligible(const GridGeom& g, uint64_t n);
-BucketBuildSizes bucket_build_sizes(const GridGeom& g, uint64_t n, int num_sms);
-int build_grid_bucketed(const float* d_xyz, uint64_t n, const GridGeom& g, int num_sms, const BucketBuildBuffers& b,
-                        cudaStream_t s);
 // cell_start[c] = first slot of cell c, from the cell ids of the sorted particles.
 int fill_cell_table(const uint32_t* sorted_cells, uint64_t n, uint64_t ncells, uint32_t* cell_start, void* gaps,
                     uint32_t* ngaps, cudaStream_t s);

@@ -1,8 +1,7 @@
-"""Grid index builds on the GPU: the two-pass bucket build (partition into
-buckets of 2^16 cells, then a counting sort of each bucket by a cluster of 8
-blocks), on dense clumps, a single crowded cell, odd and very large grids.
-The counts must equal the oracle's (which is pinned to the reference's own
-outputs)."""
+"""Grid index builds on the GPU (radix sort by cell id, then the cell-offset
+table) on dense clumps, a single crowded cell, odd and very large grids, and
+the README-scale file.  The counts must equal the oracle's (which is pinned
+to the reference's own outputs)."""
 from __future__ import annotations
 
 import numpy as np
@@ -31,8 +30,8 @@ def _halos_around(rng, centre, spread, n_near, n_far):
 
 
 def test_dense_buckets(ctx):
-    """600k particles, 80 % in a ball of radius 1: the buckets around the ball
-    hold far more records than the sort blocks keep in shared memory."""
+    """600k particles, 80 % in a ball of radius 1: a few cells hold most of
+    the particles."""
     rng = np.random.default_rng(61)
     n = 600_000
     p = rng.uniform(0, 1000, size=(n, 3))
@@ -68,9 +67,8 @@ def test_clustered_file_matches_oracle(ctx):
 
 @pytest.mark.parametrize("grid", [(2048, 512, 512), (4096, 512, 600), (1, 1, 1), (3, 1, 70001 // 3), (5, 1, 1)])
 def test_large_tiny_and_odd_grids(grid, ctx):
-    """2^29 cells (8192 buckets); more than 2^30 cells (the radix build); one
-    cell; cell counts that are not a multiple of the bucket size; buckets of
-    fewer cells than a cluster has blocks."""
+    """2^29 and more than 2^30 cells (31-bit cell ids: four 8-bit passes); one
+    cell; small and odd cell counts."""
     rng = np.random.default_rng(65)
     p = rng.uniform(0, 1000, size=(120_000, 3)).astype(np.float32)
     h = rng.uniform(0, 1000, size=(1500, 3)).astype(np.float32)
@@ -79,16 +77,16 @@ def test_large_tiny_and_odd_grids(grid, ctx):
     assert np.array_equal(_counts(ctx, p, h, r2, grid=grid, hint=12.0), oracle.count(p, h, r2))
 
 
-def test_bucket_build_at_the_automatic_readme_scale_grid(ctx):
-    """1e8 uniform particles (the README-scale file): 1000 x 400 x 400 cells,
-    28-bit cell ids, 2442 buckets sorted by clusters of 8 blocks; 20000 halos
-    including face and corner halos checked against the oracle."""
+def test_build_at_the_automatic_readme_scale_grid(ctx):
+    """1e8 uniform particles (the README-scale file): 942 x 377 x 377 cells,
+    27-bit cell ids sorted in three 9-bit passes; 20000 halos including face
+    and corner halos checked against the oracle."""
     import torch
     n = 100_000_000
     p = nat.gen_uniform_particles(1, 1, n)
     dp = torch.from_numpy(p).cuda()
     idx = ctx.build_index(dp, radius_hint=5.0)
-    assert idx.grid == (1000, 400, 400)
+    assert idx.grid == (942, 377, 377)
     rng = np.random.default_rng(66)
     h = nat.gen_uniform_halos(2, 20000)["point"].copy()
     h[:600] = rng.choice([0.0, 999.999, 1.5, 998.5, 4.99, 995.01], size=(600, 3))
