@@ -226,15 +226,17 @@ def _is_cuda(a) -> bool:
     return hasattr(a, "is_cuda") and bool(a.is_cuda)
 
 
-def _hand_over(ctx: "Context", which: int, t) -> None:
-    """Order the library's stream `which` (0 build, 1 count) after the work
-    queued on torch's current stream (the producer of tensor t), and keep t's
-    memory out of torch's allocator until the library's work queued on that
-    stream so far has finished."""
+def _hand_over(ctx: "Context", which: int, t, call) -> None:
+    """Run `call` (a library call that reads tensor t on the context's stream
+    `which`: 0 build, 1 count) ordered after the work queued on torch's
+    current stream (t's producer), and order torch's later work -- including
+    the reuse of t's memory once it is freed -- after the library's reads."""
     import torch
-    s = torch.cuda.ExternalStream(ctx.stream(which), device=t.device)
-    s.wait_stream(torch.cuda.current_stream(t.device))
-    t.record_stream(s)
+    lib_s = torch.cuda.ExternalStream(ctx.stream(which), device=t.device)
+    torch_s = torch.cuda.current_stream(t.device)
+    lib_s.wait_stream(torch_s)
+    call()
+    torch_s.wait_stream(lib_s)
 
 
 def _as_f32_xyz(a) -> np.ndarray:
@@ -309,8 +311,8 @@ class Context:
         h = _vp()
         if _is_cuda(xyz):
             n = xyz.numel() // 3
-            _hand_over(self, 0, xyz)
-            _check(lib().sjcs_index_build_device(self._h, _vp(xyz.data_ptr()), n, _c.byref(opts), _c.byref(h)))
+            _hand_over(self, 0, xyz, lambda: _check(lib().sjcs_index_build_device(
+                self._h, _vp(xyz.data_ptr()), n, _c.byref(opts), _c.byref(h))))
             keep = xyz
         else:
             arr = _as_f32_xyz(xyz)
@@ -382,9 +384,8 @@ class Context:
         if _is_cuda(halos):
             stride = 4 * (halos.shape[-1] if halos.dim() == 2 else 3)
             n = halos.shape[0] if halos.dim() == 2 else halos.numel() // 3
-            _hand_over(self, 1, halos)
-            _check(lib().sjcs_query_create_device(self._h, _vp(halos.data_ptr()), stride, n,
-                                                  _vp(r2.ctypes.data), len(r2), flags, _c.byref(h)))
+            _hand_over(self, 1, halos, lambda: _check(lib().sjcs_query_create_device(
+                self._h, _vp(halos.data_ptr()), stride, n, _vp(r2.ctypes.data), len(r2), flags, _c.byref(h))))
             keep = halos
         else:
             if isinstance(halos, np.ndarray) and halos.dtype == HALO_DTYPE:
