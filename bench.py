@@ -12,7 +12,8 @@ the build stream behind file k's count (its upload overlaps that count).
   value   halo-file passes per second (nhalos * nfiles / step time), inputs
           already resident in HBM; device time from CUDA events.
   e2e     the same through the C ABI with HOST buffers: pinned particle and
-          halo buffers copied in, uint64 counts copied back every step.
+          halo buffers copied in, the counts copied back every step (the
+          uint32 accumulators: exact while the query has not folded).
           Steps are independent jobs run as a pipeline: job k's count
           read-back (device to host) overlaps job k+1's uploads (host to
           device); every job's copies are inside the timed region.
@@ -305,8 +306,10 @@ def run_ours(args, w, dist, rank, world, local):
     halos_np = halos_pinned.numpy().view(nat.HALO_DTYPE)
     halos_np[:] = all_halos
     del all_halos
-    out_h = torch.empty((nh * nr,), dtype=torch.int64, pin_memory=True)
-    out_np = out_h.numpy().view(np.uint64).reshape(nh, nr)
+    # read-back destinations: the uint32 accumulators are the exact totals
+    # while the query has not folded (the library refuses the read otherwise)
+    out_h = torch.empty((nh * nr,), dtype=torch.int32, pin_memory=True)
+    out_np = out_h.numpy().view(np.uint32).reshape(nh, nr)
 
     ctx = nat.Context(local)
     ctx.set_overlap(args.overlap)
@@ -332,8 +335,8 @@ def run_ours(args, w, dist, rank, world, local):
             idx.destroy()
         return q
 
-    out_h2 = torch.empty((nh * nr,), dtype=torch.int64, pin_memory=True)
-    outs = [out_np, out_h2.numpy().view(np.uint64).reshape(nh, nr)]
+    out_h2 = torch.empty((nh * nr,), dtype=torch.int32, pin_memory=True)
+    outs = [out_np, out_h2.numpy().view(np.uint32).reshape(nh, nr)]
 
     def job_e2e(k):
         q = ctx.query(halos_np, r2)
@@ -341,7 +344,7 @@ def run_ours(args, w, dist, rank, world, local):
             idx = ctx.build_index(pnp[f * n:(f + 1) * n], radius_hint=R)
             q.count(idx)
             idx.destroy()
-        q.read_counts_async(outs[k & 1])
+        q.read_counts32_async(outs[k & 1])
         return q
 
     def run_e2e(jobs):
@@ -519,7 +522,7 @@ def run_ours(args, w, dist, rank, world, local):
     build_bytes = 24.0 * n + 4.0 * (ncells + 1)  # 12 B read + 12 B written per particle, 4 B per cell
     roof_build = {"bound": "hbm", "achieved": round(build_bytes / (build_ms / 1e3) / 1e9, 1), "peak": peak,
                   "unit": "GB/s", "frac": round(build_bytes / (build_ms / 1e3) / 1e9 / peak, 4),
-                  "kernel": "grid index build (radix passes k_radix_upsweep* + scan + k_radix_downsweep, k_cell_start)",
+                  "kernel": "grid index build (partition build: k_pb_top_hist, k_pb_partition x2, k_pb_mid_hist, k_pb_cells)",
                   "build_ms": round(build_ms, 3), "algorithmic_bytes_per_build": build_bytes,
                   "cells": int(ncells)}
 
@@ -539,7 +542,7 @@ def run_ours(args, w, dist, rank, world, local):
         "vs_baseline": round(value / PUBLISHED_HALO_FILES_PER_S, 2),
         "vs_baseline_ref": "reference README.md:137, 3 files x 1e7 halos in 84104 ms on 20 CPU threads",
         "dtype": "f32", "data": "synthetic: reference generator streams (MT19937 seeds 1 and 2)",
-        "config": {"workload": workload_name(w), "index": "grid (radix-sorted cell table)",
+        "config": {"workload": workload_name(w), "index": "grid (cell table, partition build)",
                    "build_kernels": "beside the counts" if args.overlap else "after the queued counts (copies overlap)",
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": f"inputs larger than L2 ({nf} x {n * 12 / 1e9:.2f} GB particle arrays per step)"},
@@ -548,7 +551,8 @@ def run_ours(args, w, dist, rank, world, local):
         "e2e": None if args.no_e2e else {
             "value": round(e2e_value, 1), "unit": UNIT, "ms_per_step": round(ms_e2e, 3),
             "h2d_bytes_per_step": int(nf * n * 12 + (nh - 1) * 24 + 12),
-            "d2h_bytes_per_step": int(nh * nr * 8),
+            "d2h_bytes_per_step": int(nh * nr * 4),
+            "read_back": "uint32 accumulators, exact without a fold (sjcs_query_read_counts32_async)",
             "pipeline": "job k's read-back overlaps job k+1's uploads (2 jobs in flight)"},
         "roofline": roof,
         "roofline_build": roof_build,

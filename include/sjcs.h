@@ -51,7 +51,7 @@ extern "C" {
 #define SJCS_ERR_STATE     4  /* object used with another context, or after destroy */
 
 /* index kinds */
-#define SJCS_INDEX_GRID     0 /* uniform cell grid: particles radix-sorted by cell, cell-offset table */
+#define SJCS_INDEX_GRID     0 /* uniform cell grid: particles grouped by cell in cell order, cell-offset table */
 #define SJCS_INDEX_LEARNED  1 /* particles sorted by 63-bit Morton key; cell ranks from a two-level
                                  piecewise-linear model (1 root + 4096 fp32 linear leaves, per-leaf
                                  max error) corrected by a bounded exact search; the Morton
@@ -298,7 +298,15 @@ int sjcs_query_read_counts(sjcs_ctx *ctx, sjcs_query *q, uint64_t *counts, int a
  * asynchronous form of sjcs_query_read_counts(..., accumulate = 0); the
  * reference reads its counts in place after the last file (main.c:651). */
 int sjcs_query_read_counts_async(sjcs_ctx *ctx, sjcs_query *q, uint64_t *counts);
-/* Block until the last read queued by sjcs_query_read_counts_async on q is in
+/* sjcs_query_read_counts_async with uint32 counts [nhalos][nrads]: a direct
+ * copy of the query's 32-bit accumulators, half the bytes of the uint64 read.
+ * Exact while the query has not folded (every count is then at most the
+ * query's bound, which stays <= 2^32 - 1 until a fold); after a fold
+ * (sjcs_query_folds > 0) it fails with SJCS_ERR_INVALID and the counts must be
+ * read as uint64.  Completion is awaited with sjcs_query_wait_read. */
+int sjcs_query_read_counts32_async(sjcs_ctx *ctx, sjcs_query *q, uint32_t *counts);
+/* Block until the last read queued by sjcs_query_read_counts_async (or its
+ * uint32 form) on q is in
  * host memory (returns at once when none is pending). */
 int sjcs_query_wait_read(sjcs_query *q);
 /* Device pointer to the query's uint32 accumulators [nhalos][nrads] in the

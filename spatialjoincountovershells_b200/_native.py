@@ -131,6 +131,7 @@ _SIGS = {
     "sjcs_ctx_prepare_files": (_c.c_int, [_vp, _u64]),
     "sjcs_query_read_counts": (_c.c_int, [_vp, _vp, _vp, _c.c_int]),
     "sjcs_query_read_counts_async": (_c.c_int, [_vp, _vp, _vp]),
+    "sjcs_query_read_counts32_async": (_c.c_int, [_vp, _vp, _vp]),
     "sjcs_query_wait_read": (_c.c_int, [_vp]),
     "sjcs_query_device_counts": (_c.c_int, [_vp, _pp]),
     "sjcs_query_set_fold_limit": (_c.c_int, [_vp, _vp, _u64]),
@@ -557,6 +558,16 @@ class Query:
             raise ValueError("out must be a C-contiguous uint64 array of nhalos*nrads elements")
         _check(lib().sjcs_query_read_counts_async(self.ctx._h, self._h, _vp(_ptr(out))))
         self._reading = out  # keep the destination alive while the copy runs
+        return out
+
+    def read_counts32_async(self, out: np.ndarray) -> np.ndarray:
+        """read_counts_async into a page-locked uint32 array: the 32-bit
+        accumulators copied as they are, exact while the query has not folded
+        (folds == 0); fails after a fold."""
+        if out.dtype != np.uint32 or not out.flags.c_contiguous or out.size != self.nhalos * self.nrads:
+            raise ValueError("out must be a C-contiguous uint32 array of nhalos*nrads elements")
+        _check(lib().sjcs_query_read_counts32_async(self.ctx._h, self._h, _vp(_ptr(out))))
+        self._reading = out
         return out
 
     def wait_read(self) -> None:

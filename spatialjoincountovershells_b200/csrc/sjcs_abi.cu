@@ -761,10 +761,10 @@ int sjcs_ctx_prepare_files(sjcs_ctx* ctx, uint64_t max_particles) {
         rc = ensure_ring(ctx);
         if (rc) return rc;
     }
-    // one file's upload (12 B), sorted particles (16 B) and sort records and
-    // keys (44 B) per particle, the tile histograms, and the largest
-    // automatic cell table (2^27 + 1 entries)
-    const uint64_t bytes = max_particles * 73ull + (134217729ull * 4ull) + (64ull << 20);
+    // one file's upload (12 B), sorted particles (16 B), the partition
+    // build's records (16 B) and middle digits (2 B) per particle, its
+    // segment tables, and the largest automatic cell table (2^28 + 1 entries)
+    const uint64_t bytes = max_particles * 48ull + (268435457ull * 4ull) + (64ull << 20);
     return max_particles ? sjcs_ctx_reserve(ctx, bytes) : SJCS_OK;
 }
 
@@ -1357,6 +1357,32 @@ int sjcs_query_read_counts_async(sjcs_ctx* ctx, sjcs_query* q, uint64_t* counts)
     k_widen_u32_u64<<<ctx->num_sms * 8, 256, 0, s>>>(q->counts, m, q->counts64, wide);
     SJCS_LAUNCH_CHECK();
     SJCS_CUDA_TRY(cudaMemcpyAsync(counts, wide, m * sizeof(uint64_t), cudaMemcpyDeviceToHost, s));
+    SJCS_CUDA_TRY(cudaEventRecord(q->ev_d1, s));
+    q->read_queued = true;
+    return SJCS_OK;
+}
+
+int sjcs_query_read_counts32_async(sjcs_ctx* ctx, sjcs_query* q, uint32_t* counts) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_query(q) || q->ctx != ctx) return fail(SJCS_ERR_STATE, "query does not belong to this context");
+    const uint64_t m = q->nhalos * (uint64_t)q->nrads;
+    if (m == 0) return SJCS_OK;
+    if (!counts) return fail(SJCS_ERR_INVALID, "counts is NULL");
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    if (!is_pinned(counts) || !is_pinned(counts + (m - 1)))
+        return fail(SJCS_ERR_INVALID, "counts must be page-locked host memory for an asynchronous read");
+    std::lock_guard<std::mutex> lk(ctx->mu);
+    // without a fold every accumulated count is <= the query's bound <=
+    // 2^32 - 1, so the 32-bit accumulators are the totals themselves
+    if (q->folds)
+        return fail(SJCS_ERR_INVALID, "the counts were folded into 64-bit totals %u time(s): read them as uint64",
+                    q->folds);
+    cudaStream_t s = ctx->s_read;
+    SJCS_CUDA_TRY(cudaEventRecord(q->ev_rq, ctx->s_count));
+    SJCS_CUDA_TRY(cudaStreamWaitEvent(s, q->ev_rq, 0));
+    SJCS_CUDA_TRY(cudaEventRecord(q->ev_d0, s));
+    SJCS_CUDA_TRY(cudaMemcpyAsync(counts, q->counts, m * sizeof(uint32_t), cudaMemcpyDeviceToHost, s));
     SJCS_CUDA_TRY(cudaEventRecord(q->ev_d1, s));
     q->read_queued = true;
     return SJCS_OK;

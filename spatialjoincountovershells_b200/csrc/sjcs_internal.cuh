@@ -267,7 +267,8 @@ int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx
 int exclusive_scan_u32(uint32_t* d_data, uint64_t m, cudaStream_t s, uint32_t* partials = nullptr);
 uint64_t scan_partials_needed(uint64_t m);
 
-// index_build.cu: the grid build on caller-provided buffers (no allocation).
+// index_build.cu: the stable LSD grid build on caller-provided buffers (no
+// allocation; the fixed-buffer entry point and cell keys of more than 30 bits).
 struct GridBuildBuffers {
     float4* pts;          // n sorted particles (output)
     uint32_t* cell_start; // ncells + 1 (output)
@@ -284,7 +285,7 @@ struct GridBuildBuffers {
 };
 constexpr uint32_t kGridGaps = 1u << 16;
 int grid_key_bits(const GridGeom& g);
-int grid_digit_bits(const GridGeom& g);  // 9 for 25-27-bit cell keys, else 8
+int grid_digit_bits(const GridGeom& g);  // LSD build: 9 for 25-27-bit cell keys, else 8
 int build_grid_into(const float* d_xyz, uint64_t n, const GridGeom& g, const GridBuildBuffers& b, cudaStream_t s);
 // cell_start[c] = first slot of cell c, from the cell ids of the sorted particles.
 int fill_cell_table(const uint32_t* sorted_cells, uint64_t n, uint64_t ncells, uint32_t* cell_start, void* gaps,

@@ -78,15 +78,16 @@ def test_large_tiny_and_odd_grids(grid, ctx):
 
 
 def test_build_at_the_automatic_readme_scale_grid(ctx):
-    """1e8 uniform particles (the README-scale file): 942 x 377 x 377 cells,
-    27-bit cell ids sorted in three 9-bit passes; 20000 halos including face
-    and corner halos checked against the oracle."""
+    """1e8 uniform particles (the README-scale file): 1000 x 400 x 400 cells
+    (28-bit cell ids: segments of 1024 cells under two 9-bit partition
+    passes); 20000 halos including face and corner halos checked against the
+    oracle."""
     import torch
     n = 100_000_000
     p = nat.gen_uniform_particles(1, 1, n)
     dp = torch.from_numpy(p).cuda()
     idx = ctx.build_index(dp, radius_hint=5.0)
-    assert idx.grid == (942, 377, 377)
+    assert idx.grid == (1000, 400, 400)
     rng = np.random.default_rng(66)
     h = nat.gen_uniform_halos(2, 20000)["point"].copy()
     h[:600] = rng.choice([0.0, 999.999, 1.5, 998.5, 4.99, 995.01], size=(600, 3))

@@ -69,6 +69,32 @@ def test_folds_keep_totals_exact_across_many_files(many_files, ctx, sched):
     q.destroy()
 
 
+def test_uint32_read_is_exact_until_a_fold(many_files, ctx):
+    """The uint32 read-back copies the accumulators as they are: equal to the
+    oracle's totals while no fold has happened, refused after one."""
+    files, h, r2, per_file = many_files
+    q = ctx.query(h, r2)
+    q.set_fold_limit(70000)
+    buf = nat.PinnedBuffer((len(h), len(r2)), np.uint32)
+    for k in range(2):
+        idx = ctx.build_index(files[k], radius_hint=20.0)
+        q.count(idx)
+        idx.destroy()
+    assert q.folds == 0
+    q.read_counts32_async(buf.array)
+    q.wait_read()
+    assert np.array_equal(buf.array, per_file[0] + per_file[1])
+    idx = ctx.build_index(files[2], radius_hint=20.0)
+    q.count(idx)
+    idx.destroy()
+    assert q.folds == 1
+    with pytest.raises(nat.SjcsError):
+        q.read_counts32_async(buf.array)
+    assert np.array_equal(q.read_counts(), sum(per_file[:3]))
+    buf.free()
+    q.destroy()
+
+
 def test_fold_with_radius_beyond_half_box(ctx):
     """R >= 499: a particle can lie in several images' boxes, so one file may add
     8n to an accumulator; the query folds on that bound."""
