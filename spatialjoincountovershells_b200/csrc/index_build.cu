@@ -127,8 +127,8 @@ __global__ void k_fill_gaps(const Gap* __restrict__ gaps, const uint32_t* __rest
 // cell-table entries itself:
 //   top     counts of the key's top digit (<= 9 bits) over x,y,z, in shared
 //           memory; their prefix starts the top buckets
-//   pass A  x,y,z records by the top digit, and beside them the next digit
-//           (16 bits per record)
+//   pass A  x,y,z -> (x, y, z, key) records by the top digit, and beside them
+//           the next digit (16 bits per record)
 //   mid     per tile of a top bucket: counts of the next digit in shared
 //           memory, added to the segment counts (a segment is 2^sb cells,
 //           sb = max(9, key bits - 18) <= 12); their prefix starts the segments
@@ -136,10 +136,9 @@ __global__ void k_fill_gaps(const Gap* __restrict__ gaps, const uint32_t* __rest
 //           (keys of more than sb + 9 bits; else the top digit is the segment)
 //   cells   per group of 4096 cells (whole segments): cell counts, cell_start
 //           of its cells, records written in cell order
-// Records between the passes are the particles' 12 bytes (every pass stages
-// its tile in shared memory and computes the keys again); the sorted
-// particles are float4 with the cell key in .w, which the count kernel does
-// not read.
+// Records are 16 bytes with the cell key in .w, which the count kernel does
+// not read.  (12-byte records, keys computed again in every pass, were
+// measured slower: a record then leaves as three scattered 4-byte stores.)
 constexpr int PB_THREADS = 512;
 constexpr int PB_ITEMS = 8;
 constexpr uint32_t PB_TILE = PB_THREADS * PB_ITEMS;  // records per block in a partition pass
@@ -251,24 +250,40 @@ k_pb_tiles(const uint32_t* __restrict__ top_start, uint32_t ntop, PbTile* __rest
 }
 
 // Segment counts for the middle pass: block i counts the middle digits of
-// tile i (mid[] as written by pass A) in shared memory and adds them to
-// seg_hist[(bucket << bits_mid) + digit] -- one reduction per (tile, digit)
-// instead of one per record.
+// tiles 8i .. 8i+7 (mid[] as written by pass A) in shared memory and adds
+// them to seg_hist[(bucket << bits_mid) + digit] whenever the bucket changes
+// and at the end -- a reduction per (bucket run, digit) rather than per
+// record.
+constexpr uint32_t PB_MID_TILES = 8;
 __global__ void __launch_bounds__(PB_THREADS)
 k_pb_mid_hist(const uint16_t* __restrict__ mid, const PbTile* __restrict__ tiles,
               const uint32_t* __restrict__ ntiles, int bits_mid, uint64_t nseg, uint32_t* __restrict__ seg_hist) {
     __shared__ uint32_t sh[PB_THREADS];
-    if (blockIdx.x >= *ntiles) return;
-    const PbTile tl = tiles[blockIdx.x];
-    sh[threadIdx.x] = 0u;
-    __syncthreads();
+    const uint32_t nt = *ntiles, t0 = blockIdx.x * PB_MID_TILES;
+    if (t0 >= nt) return;
+    const uint32_t t1 = min(t0 + PB_MID_TILES, nt);
     // masked: a slot that pass A left unwritten (only if the input changed
     // after the histogram) cannot index out of range
     const uint32_t mask = (1u << bits_mid) - 1u;
-    for (uint32_t j = threadIdx.x; j < tl.len; j += PB_THREADS) atomicAdd(&sh[mid[tl.start + j] & mask], 1u);
+    sh[threadIdx.x] = 0u;
+    uint32_t bucket = tiles[t0].bucket;
+    __syncthreads();
+    for (uint32_t t = t0; t < t1; ++t) {
+        const PbTile tl = tiles[t];
+        if (tl.bucket != bucket) {  // uniform across the block
+            __syncthreads();
+            const uint32_t c = sh[threadIdx.x];
+            const uint64_t sg = ((uint64_t)bucket << bits_mid) + threadIdx.x;
+            if (c && sg < nseg) atomicAdd(&seg_hist[sg], c);
+            sh[threadIdx.x] = 0u;
+            bucket = tl.bucket;
+            __syncthreads();
+        }
+        for (uint32_t j = threadIdx.x; j < tl.len; j += PB_THREADS) atomicAdd(&sh[mid[tl.start + j] & mask], 1u);
+    }
     __syncthreads();
     const uint32_t c = sh[threadIdx.x];
-    const uint64_t sg = ((uint64_t)tl.bucket << bits_mid) + threadIdx.x;
+    const uint64_t sg = ((uint64_t)bucket << bits_mid) + threadIdx.x;
     if (c && sg < nseg) atomicAdd(&seg_hist[sg], c);
 }
 
@@ -293,19 +308,18 @@ __device__ __forceinline__ uint32_t pb_stage(const float* __restrict__ base, int
     return (uint32_t)(w_src - a0);
 }
 
-// One partition pass over 12-byte (x, y, z) records.  kTiles == false: tile
-// blockIdx.x of the input (the first pass over the caller's particles);
-// otherwise tile blockIdx.x of `tiles`.  Keys are computed from x, y, z.  A
-// record's digit is (key >> shift) & (2^bits - 1) and its room is reserved
-// from cursors[(bucket << cur_shift) + digit]; it leaves as 12 bytes at
-// out[3 * slot].  With `mid` given, the pass also writes mid[slot] = (key >>
-// sb) & mid_mask beside every record.
+// One partition pass.  kTiles == false: tile blockIdx.x of the caller's
+// x,y,z (the first pass; staged in shared memory, keys computed here);
+// otherwise tile blockIdx.x of `tiles` over 16-byte (x, y, z, key) records.
+// A record's digit is (key >> shift) & (2^bits - 1) and its room is reserved
+// from cursors[(bucket << cur_shift) + digit].  With `mid` given, the pass
+// also writes mid[slot] = (key >> sb) & mid_mask beside every record.
 template <bool kTiles>
 __global__ void __launch_bounds__(PB_THREADS, 2)
-k_pb_partition(const float* __restrict__ in, int in_aligned, const PbTile* __restrict__ tiles,
-               const uint32_t* __restrict__ ntiles, uint64_t n, GridGeom g, int shift, int bits, int cur_shift,
-               uint32_t* __restrict__ cursors, float* __restrict__ out, uint16_t* __restrict__ mid, int sb,
-               uint32_t mid_mask) {
+k_pb_partition(const float* __restrict__ xyz, int xyz_aligned, const float4* __restrict__ in,
+               const PbTile* __restrict__ tiles, const uint32_t* __restrict__ ntiles, uint64_t n, GridGeom g,
+               int shift, int bits, int cur_shift, uint32_t* __restrict__ cursors, float4* __restrict__ out,
+               uint16_t* __restrict__ mid, int sb, uint32_t mid_mask) {
     __shared__ uint32_t cnt[PB_THREADS];  // one bin per thread (digits of <= 9 bits)
     __shared__ uint32_t dstart[PB_THREADS];
     __shared__ uint32_t delta[PB_THREADS];
@@ -328,23 +342,35 @@ k_pb_partition(const float* __restrict__ in, int in_aligned, const PbTile* __res
         bucket = tl.bucket;
     }
     cnt[tid] = 0;
-    float* sx = reinterpret_cast<float*>(xch);
-    const uint32_t off = pb_stage(in, in_aligned, 3 * start, 3u * len, 3 * n, sx);
-    cp_async_wait_all();
-    __syncthreads();
     float4 v[PB_ITEMS];
+    if constexpr (!kTiles) {
+        float* sx = reinterpret_cast<float*>(xch);
+        const uint32_t off = pb_stage(xyz, xyz_aligned, 3 * start, 3u * len, 3 * n, sx);
+        cp_async_wait_all();
+        __syncthreads();
+#pragma unroll
+        for (int i = 0; i < PB_ITEMS; ++i) {
+            const uint32_t loc = (uint32_t)i * PB_THREADS + (uint32_t)tid;
+            if (loc < len) {
+                const float x = sx[off + 3 * loc], y = sx[off + 3 * loc + 1], z = sx[off + 3 * loc + 2];
+                v[i] = make_float4(x, y, z, __uint_as_float(cell_key(g, x, y, z)));
+            }
+        }
+    } else {
+#pragma unroll
+        for (int i = 0; i < PB_ITEMS; ++i) {
+            const uint32_t loc = (uint32_t)i * PB_THREADS + (uint32_t)tid;
+            if (loc < len) v[i] = in[start + loc];
+        }
+        __syncthreads();
+    }
     uint32_t r[PB_ITEMS];
 #pragma unroll
     for (int i = 0; i < PB_ITEMS; ++i) {
         const uint32_t loc = (uint32_t)i * PB_THREADS + (uint32_t)tid;
-        if (loc < len) {
-            const float x = sx[off + 3 * loc], y = sx[off + 3 * loc + 1], z = sx[off + 3 * loc + 2];
-            const uint32_t key = cell_key(g, x, y, z);
-            v[i] = make_float4(x, y, z, __uint_as_float(key));
-            r[i] = atomicAdd(&cnt[(key >> shift) & mask], 1u);
-        }
+        if (loc < len) r[i] = atomicAdd(&cnt[(pb_key(v[i]) >> shift) & mask], 1u);
     }
-    __syncthreads();  // ranks done; the staged records are no longer read
+    __syncthreads();  // ranks done; the staged x,y,z are no longer read
     const uint32_t c = cnt[tid];
     uint32_t gb = 0, total;
     if (c) gb = atomicAdd(&cursors[((uint64_t)bucket << cur_shift) + (uint64_t)tid], c);
@@ -365,31 +391,21 @@ k_pb_partition(const float* __restrict__ in, int in_aligned, const PbTile* __res
             const float4 w = xch[j];
             const uint32_t o = delta[(pb_key(w) >> shift) & mask] + j;
             if (o < n) {  // in range unless the input changed after the histogram
-                float* dst = out + 3ull * o;
-                dst[0] = w.x;
-                dst[1] = w.y;
-                dst[2] = w.z;
+                out[o] = w;
                 if (mid) mid[o] = (uint16_t)((pb_key(w) >> sb) & mid_mask);
             }
         }
     }
 }
 
-// Last pass: block b counting-sorts the 12-byte records of cells [4096 b,
-// 4096 b + 4096) (whole segments of 2^sb cells, contiguous after the
-// partition passes), writes cell_start for those of its cells that are <=
-// ncells and the particles as float4 (x, y, z, key).  A group of at most
-// PB_TILE records is staged in shared memory; a larger one is read twice
-// (counts, then placement) and written in place.
-__device__ __forceinline__ float4 pb_record(const GridGeom& g, const float* __restrict__ r) {
-    const float x = r[0], y = r[1], z = r[2];
-    return make_float4(x, y, z, __uint_as_float(cell_key(g, x, y, z)));
-}
-
+// Last pass: block b counting-sorts the records of cells [4096 b, 4096 b +
+// 4096) (whole segments of 2^sb cells, contiguous after the partition passes)
+// and writes cell_start for those of its cells that are <= ncells.  A group
+// of at most PB_TILE records goes through shared memory; a larger one is read
+// twice (counts, then placement) and written in place.
 __global__ void __launch_bounds__(PB_THREADS, 2)
-k_pb_cells(const float* __restrict__ in, uint64_t n, GridGeom g, const uint32_t* __restrict__ seg_start,
-           uint64_t nseg, int sb, uint32_t* __restrict__ cs, float4* __restrict__ out) {
-    const uint64_t ncells = g.ncells;
+k_pb_cells(const float4* __restrict__ in, const uint32_t* __restrict__ seg_start, uint64_t nseg, int sb,
+           uint64_t ncells, uint32_t* __restrict__ cs, float4* __restrict__ out) {
     __shared__ __align__(16) uint32_t hist[PB_GROUP_CELLS];
     __shared__ uint32_t ws[PB_THREADS / 32 + 1];
     extern __shared__ float4 xch[];
@@ -406,18 +422,20 @@ k_pb_cells(const float* __restrict__ in, uint64_t n, GridGeom g, const uint32_t*
     const bool fits = cnt <= PB_TILE;
     float4 v[PB_ITEMS];
     uint32_t r[PB_ITEMS];
-    uint32_t off = 0;
-    if (fits) off = pb_stage(in, 1, 3ull * lo, 3u * cnt, 3 * n, reinterpret_cast<float*>(xch));
-    cp_async_wait_all();
+    if (fits) {
+#pragma unroll
+        for (int i = 0; i < PB_ITEMS; ++i) {
+            const uint32_t j = (uint32_t)i * PB_THREADS + (uint32_t)tid;
+            if (j < cnt) v[i] = in[lo + j];
+        }
+    }
     __syncthreads();
     if (fits) {
-        const float* sx = reinterpret_cast<const float*>(xch) + off;
 #pragma unroll
         for (int i = 0; i < PB_ITEMS; ++i) {
             const uint32_t j = (uint32_t)i * PB_THREADS + (uint32_t)tid;
             r[i] = 0xffffffffu;
             if (j < cnt) {
-                v[i] = pb_record(g, sx + 3 * j);
                 // a key outside the group (only if the input changed after the
                 // histogram) is dropped rather than counted out of range
                 const uint32_t lk = pb_key(v[i]) - c0;
@@ -426,7 +444,7 @@ k_pb_cells(const float* __restrict__ in, uint64_t n, GridGeom g, const uint32_t*
         }
     } else {
         for (uint32_t j = (uint32_t)tid; j < cnt; j += PB_THREADS) {
-            const uint32_t lk = pb_key(pb_record(g, in + 3ull * (lo + j))) - c0;
+            const uint32_t lk = pb_key(in[lo + j]) - c0;
             if (lk < PB_GROUP_CELLS) atomicAdd(&hist[lk], 1u);
         }
     }
@@ -458,7 +476,7 @@ k_pb_cells(const float* __restrict__ in, uint64_t n, GridGeom g, const uint32_t*
         for (int k = 0; k < 8; ++k)
             if (c8 + k <= ncells) cs[c8 + k] = lo + e[k];
     }
-    __syncthreads();  // also: the staged records are no longer read
+    __syncthreads();
     if (fits) {
 #pragma unroll
         for (int i = 0; i < PB_ITEMS; ++i) {
@@ -472,7 +490,7 @@ k_pb_cells(const float* __restrict__ in, uint64_t n, GridGeom g, const uint32_t*
         }
     } else {
         for (uint32_t j = (uint32_t)tid; j < cnt; j += PB_THREADS) {
-            const float4 w = pb_record(g, in + 3ull * (lo + j));
+            const float4 w = in[lo + j];
             const uint32_t lk = pb_key(w) - c0;
             if (lk < PB_GROUP_CELLS) out[lo + atomicAdd(&hist[lk], 1u)] = w;
         }
@@ -500,14 +518,14 @@ int build_grid_partitioned(const float* d_xyz, uint64_t n, const GridGeom& g, fl
 
     StreamScratch scr(s);
     uint32_t *top = nullptr, *cur_top = nullptr, *seg = nullptr, *cur_seg = nullptr, *ntiles = nullptr;
-    float* tmp = nullptr;  // 12-byte records
+    float4* tmp = nullptr;
     PbTile* tiles = nullptr;
     uint16_t* mid = nullptr;
     // top digit counts and starts (ntop + 1 entries); without a middle pass
     // the top digit is the segment and these are the segment starts too
     SJCS_CUDA_TRY(scr.alloc(&top, ((uint64_t)ntop + 1) * sizeof(uint32_t)));
     SJCS_CUDA_TRY(scr.alloc(&cur_top, (uint64_t)ntop * sizeof(uint32_t)));
-    SJCS_CUDA_TRY(scr.alloc(&tmp, n * 3 * sizeof(float)));
+    SJCS_CUDA_TRY(scr.alloc(&tmp, n * sizeof(float4)));
     if (bits_mid) {
         SJCS_CUDA_TRY(scr.alloc(&seg, (nseg + 1) * sizeof(uint32_t)));
         SJCS_CUDA_TRY(scr.alloc(&cur_seg, nseg * sizeof(uint32_t)));
@@ -534,26 +552,26 @@ int build_grid_partitioned(const float* d_xyz, uint64_t n, const GridGeom& g, fl
     SJCS_CUDA_TRY(cudaFuncSetAttribute(k_pb_cells, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)PB_SMEM));
     // pass A writes pts when a middle pass follows (pts is free until the
     // last pass), else tmp; with a middle pass it also writes the middle digits
-    float* a_out = bits_mid ? reinterpret_cast<float*>(pts) : tmp;
+    float4* a_out = bits_mid ? pts : tmp;
     const uint32_t mid_mask = (1u << bits_mid) - 1u;
     k_pb_partition<false><<<(unsigned)ntiles_in, PB_THREADS, PB_SMEM, s>>>(
-        d_xyz, aligned, nullptr, nullptr, n, g, top_shift, bits_top, 0, cur_top, a_out, mid, sb, mid_mask);
+        d_xyz, aligned, nullptr, nullptr, nullptr, n, g, top_shift, bits_top, 0, cur_top, a_out, mid, sb, mid_mask);
     SJCS_LAUNCH_CHECK();
     if (bits_mid) {
         const unsigned tile_blocks = (unsigned)((ntiles_mid + PB_THREADS - 1) / PB_THREADS);
         k_pb_tiles<<<tile_blocks, PB_THREADS, 0, s>>>(top, ntop, tiles, ntiles);
         SJCS_LAUNCH_CHECK();
-        k_pb_mid_hist<<<(unsigned)ntiles_mid, PB_THREADS, 0, s>>>(mid, tiles, ntiles, bits_mid, nseg, seg);
+        k_pb_mid_hist<<<(unsigned)((ntiles_mid + PB_MID_TILES - 1) / PB_MID_TILES), PB_THREADS, 0, s>>>(
+            mid, tiles, ntiles, bits_mid, nseg, seg);
         SJCS_LAUNCH_CHECK();
         rc = exclusive_scan_u32(seg, nseg + 1, s);
         if (rc) return rc;
         SJCS_CUDA_TRY(cudaMemcpyAsync(cur_seg, seg, nseg * sizeof(uint32_t), cudaMemcpyDeviceToDevice, s));
         k_pb_partition<true><<<(unsigned)ntiles_mid, PB_THREADS, PB_SMEM, s>>>(
-            reinterpret_cast<const float*>(pts), 1, tiles, ntiles, n, g, sb, bits_mid, bits_mid, cur_seg, tmp,
-            nullptr, sb, 0u);
+            nullptr, 0, pts, tiles, ntiles, n, g, sb, bits_mid, bits_mid, cur_seg, tmp, nullptr, sb, 0u);
         SJCS_LAUNCH_CHECK();
     }
-    k_pb_cells<<<(unsigned)ngroups, PB_THREADS, PB_SMEM, s>>>(tmp, n, g, seg, nseg, sb, cs, pts);
+    k_pb_cells<<<(unsigned)ngroups, PB_THREADS, PB_SMEM, s>>>(tmp, seg, nseg, sb, g.ncells, cs, pts);
     SJCS_LAUNCH_CHECK();
     return SJCS_OK;
 }

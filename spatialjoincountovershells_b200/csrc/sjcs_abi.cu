@@ -147,6 +147,34 @@ void build_shell_lut(const float* r2, int nrads, std::vector<uint32_t>* lut, uin
 
 }  // namespace
 
+constexpr uint32_t kParamSlots = 8;
+constexpr size_t kParamSlotBytes = 64 << 10;
+
+// Copy `bytes` of host memory to dst on stream s without the host waiting for
+// s: through a page-locked slot of the context (the slot's previous copy is
+// long done unless 8 newer ones are still queued); larger tables fall back to
+// a pageable copy.
+int upload_params(sjcs_ctx* ctx, void* dst, const void* src, size_t bytes, cudaStream_t s) {
+    if (bytes == 0) return SJCS_OK;
+    if (bytes > kParamSlotBytes) {
+        SJCS_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s));
+        return SJCS_OK;
+    }
+    std::lock_guard<std::mutex> lk(ctx->param_mu);
+    if (!ctx->param_ring) {
+        SJCS_CUDA_TRY(cudaMallocHost(&ctx->param_ring, kParamSlots * kParamSlotBytes));
+        ctx->param_ev.assign(kParamSlots, nullptr);
+        for (auto& e : ctx->param_ev) SJCS_CUDA_TRY(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+    }
+    const uint32_t slot = ctx->param_next++ % kParamSlots;
+    char* p = ctx->param_ring + (size_t)slot * kParamSlotBytes;
+    SJCS_CUDA_TRY(cudaEventSynchronize(ctx->param_ev[slot]));
+    std::memcpy(p, src, bytes);
+    SJCS_CUDA_TRY(cudaMemcpyAsync(dst, p, bytes, cudaMemcpyHostToDevice, s));
+    SJCS_CUDA_TRY(cudaEventRecord(ctx->param_ev[slot], s));
+    return SJCS_OK;
+}
+
 int query_prepare(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride, uint64_t nhalos, const float* r2,
                   int nrads, int flags, sjcs_query* q, cudaStream_t s) {
     q->nhalos = nhalos;
@@ -167,14 +195,15 @@ int query_prepare(sjcs_ctx* ctx, const float* d_halo_xyz, size_t stride, uint64_
     SJCS_CUDA_TRY(cudaMallocAsync(&q->d_r2, (size_t)pad * sizeof(float), s));
     k_fill_f32<<<(pad + 255) / 256, 256, 0, s>>>(q->d_r2, (uint64_t)pad, INFINITY);
     SJCS_LAUNCH_CHECK();
-    SJCS_CUDA_TRY(cudaMemcpyAsync(q->d_r2, r2, (size_t)nrads * sizeof(float), cudaMemcpyHostToDevice, s));
+    int rc = upload_params(ctx, q->d_r2, r2, (size_t)nrads * sizeof(float), s);
+    if (rc) return rc;
     std::vector<uint32_t> lut;
     if (mono) build_shell_lut(r2, nrads, &lut, &q->lut_k0, &q->lut_shift);
     q->nlut = (int)lut.size();
     if (!lut.empty()) {
         SJCS_CUDA_TRY(cudaMallocAsync(&q->d_lut, lut.size() * sizeof(uint32_t), s));
-        SJCS_CUDA_TRY(cudaMemcpyAsync(q->d_lut, lut.data(), lut.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s));
-        // the pageable source is copied before cudaMemcpyAsync returns
+        rc = upload_params(ctx, q->d_lut, lut.data(), lut.size() * sizeof(uint32_t), s);
+        if (rc) return rc;
     }
     const uint64_t ncnt = nhalos * (uint64_t)nrads;
     SJCS_CUDA_TRY(cudaMallocAsync(&q->counts, (ncnt ? ncnt : 1) * sizeof(uint32_t), s));
@@ -557,6 +586,9 @@ int sjcs_ctx_destroy(sjcs_ctx* ctx) {
     for (cudaEvent_t e : ctx->ring_ev)
         if (e) cudaEventDestroy(e);
     if (ctx->ring) cudaFreeHost(ctx->ring);
+    for (cudaEvent_t e : ctx->param_ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->param_ring) cudaFreeHost(ctx->param_ring);
     if (ctx->ev_counts) cudaEventDestroy(ctx->ev_counts);
     ctx->magic = 0;
     delete ctx;

@@ -131,6 +131,13 @@ struct sjcs_ctx {
     std::mutex ring_mu;
     char* ring = nullptr;
     std::vector<cudaEvent_t> ring_ev;
+    // Small parameter uploads (radius and shell tables): page-locked slots,
+    // each with the event of the last copy out of it, because a copy from
+    // pageable memory may make the host wait for its stream.
+    std::mutex param_mu;
+    char* param_ring = nullptr;
+    std::vector<cudaEvent_t> param_ev;
+    uint32_t param_next = 0;
 };
 
 namespace sjcs {
