@@ -171,6 +171,47 @@ def test_no_alloc_edge_inputs_match_the_allocating_path():
         assert bool((dc == 3).all())
 
 
+def test_no_alloc_call_replays_from_a_cuda_graph():
+    """A call captured into a CUDA graph (after the warm-up call that loads the
+    scratch array) replays with its radius table baked into the graph: each
+    replay adds the same counts as a direct call, the oracle-pinned
+    allocating path's."""
+    import torch
+    with nat.Context(0) as ctx:
+        rng = np.random.default_rng(27)
+        n, m = 60000, 2500
+        p = rng.uniform(0, 1000, size=(n, 3)).astype(np.float32)
+        h = rng.uniform(0, 1000, size=(m, 3)).astype(np.float32)
+        h[:30] = rng.choice([0.0, 999.99, 4.0, 996.0], size=(30, 3))
+        r2 = nat.radius_table(0.05, 30.0, 24)
+        nr = len(r2)
+        dp = torch.from_numpy(p).cuda()
+        dh = torch.from_numpy(h).cuda()
+        dcounts = torch.zeros(m * nr, dtype=torch.int32, device="cuda")
+        want = _allocating_path(ctx, dp, dh, r2, True)
+        side = torch.cuda.Stream()
+        side.wait_stream(torch.cuda.current_stream())
+        with torch.cuda.stream(side):
+            assert _noalloc(dp, dh, r2, dcounts, stream=side.cuda_stream) == 0, nat.lib().sjcs_last_error()
+        side.synchronize()
+        assert np.array_equal(_u32_counts(dcounts, m, nr), want)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph, stream=side):
+            rc = _noalloc(dp, dh, r2, dcounts, stream=side.cuda_stream)
+        assert rc == 0, nat.lib().sjcs_last_error()
+        # the table the graph holds must not depend on this host array
+        r2[:] = np.float32(1.0)
+        dcounts.zero_()
+        torch.cuda.synchronize()
+        graph.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(_u32_counts(dcounts, m, nr), want)
+        graph.replay()
+        torch.cuda.synchronize()
+        assert np.array_equal(_u32_counts(dcounts, m, nr), 2 * want)
+        del graph
+
+
 def test_no_alloc_rejects_sizes_beyond_its_limits():
     import torch
     r2 = nat.radius_table(0.01, 5.0, 8)
