@@ -101,7 +101,7 @@ typedef struct sjcs_learned_info {
     double   mean_err;    /* mean error bound over non-empty leaves */
     uint64_t checked;     /* cell boundaries judged against the table (0 without SJCS_INDEX_VERIFY) */
     uint64_t mismatches;  /* judged lookups that disagreed (> 0: the index answers from the table) */
-    float    sort_ms;     /* key, radix sort and offset table kernels */
+    float    sort_ms;     /* key, sort and offset table kernels */
     float    train_ms;    /* training (and judge) kernels */
 } sjcs_learned_info;
 
@@ -112,7 +112,7 @@ typedef struct sjcs_learned_info {
  * last read-back. */
 typedef struct sjcs_timing {
     float h2d_ms;         /* host-to-device copy inside the call */
-    float build_ms;       /* index build kernels (key, radix sort, gather, offsets) */
+    float build_ms;       /* index build kernels (keys, sort or partition, offsets) */
     float count_ms;       /* shell-count kernel(s) */
     float d2h_ms;         /* device-to-host read-back (widening kernel + copy) */
     uint32_t count_calls; /* number of sjcs_query_count calls summed in count_ms */
