@@ -17,9 +17,11 @@ the build stream behind file k's count (its upload overlaps that count).
           Steps are independent jobs run as a pipeline: job k's count
           read-back (device to host) overlaps job k+1's uploads (host to
           device); every job's copies are inside the timed region.
-  roofline  the shell-count kernel: algorithmic bytes per halo-file
-          (12 + 8*nrads + 12*density*(2R)^3 = 1532 B) x halos per launch
-          over its average launch time (CUDA events on the count stream).
+  roofline  the shell-count kernel (the fused k_shell_count_multi: one launch
+          counts the step's halos against all its files): algorithmic bytes
+          per halo-file (12 + 8*nrads + 12*density*(2R)^3 = 1532 B) x
+          halo-files per launch over its average launch time (CUDA events on
+          the count stream).
   cpu_baseline  the reference program (oracle/_ref/astr_rcount.exe) on a
           bounded sample of the same workload on this host's cores.
 
@@ -264,13 +266,14 @@ def parity_record(ref_counts, forms: dict, workload: str, radius) -> dict:
 # our arm
 # ---------------------------------------------------------------------------
 
-def profile_traffic(nhalos: int):
-    """DRAM bytes per count launch from the committed ncu summary, scaled to nhalos."""
-    p = ROOT / "profiles" / "shell_count_uniform.md"
+def profile_traffic(halo_files: float, fused: bool = False):
+    """DRAM bytes per count launch from the committed ncu summary of that
+    kernel (bytes per halo-file), scaled to the launch's halo-files."""
+    p = ROOT / "profiles" / ("shell_count_multi_uniform.md" if fused else "shell_count_uniform.md")
     if not p.exists():
         return None
     m = re.search(r"dram_bytes_per_halo_file:\s*([0-9.eE+]+)", p.read_text())
-    return float(m.group(1)) * nhalos if m else None
+    return float(m.group(1)) * halo_files if m else None
 
 
 def measured_peak():
@@ -314,11 +317,11 @@ def run_ours(args, w, dist, rank, world, local):
     ctx = nat.Context(local)
     ctx.set_overlap(args.overlap)
     # grow the device pool once, so no step takes new memory from the driver:
-    # 3 queries, a read-back's widened counts, 4 indexes, the uploaded files
-    # and one build's scratch
+    # 3 queries, a read-back's widened counts, two jobs' indexes, the uploaded
+    # files and one build's scratch
     idx_bytes = n * 16 + int(1.6 * n + 4096) * 4
     if not args.no_reserve:
-        ctx.reserve(3 * nh * (16 + 4 * nr + 48) + nh * nr * 8 + 4 * idx_bytes + nf * n * 12 + n * 44 + (1 << 30))
+        ctx.reserve(3 * nh * (16 + 4 * nr + 48) + nh * nr * 8 + 2 * nf * idx_bytes + nf * n * 12 + n * 44 + (1 << 30))
     s_build = torch.cuda.ExternalStream(ctx.stream(0))
     s_count = torch.cuda.ExternalStream(ctx.stream(1))
 
@@ -328,10 +331,11 @@ def run_ours(args, w, dist, rank, world, local):
     torch.cuda.synchronize()
 
     def step_resident():
+        # every file's index, then one fused count over them (sjcs_query_count_many)
         q = ctx.query(halos_d, r2)
-        for f in range(nf):
-            idx = ctx.build_index(parts_d[f], radius_hint=R)
-            q.count(idx)
+        idxs = [ctx.build_index(parts_d[f], radius_hint=R) for f in range(nf)]
+        q.count_many(idxs)
+        for idx in idxs:
             idx.destroy()
         return q
 
@@ -340,9 +344,9 @@ def run_ours(args, w, dist, rank, world, local):
 
     def job_e2e(k):
         q = ctx.query(halos_np, r2)
-        for f in range(nf):
-            idx = ctx.build_index(pnp[f * n:(f + 1) * n], radius_hint=R)
-            q.count(idx)
+        idxs = [ctx.build_index(pnp[f * n:(f + 1) * n], radius_hint=R) for f in range(nf)]
+        q.count_many(idxs)
+        for idx in idxs:
             idx.destroy()
         q.read_counts32_async(outs[k & 1])
         return q
@@ -395,6 +399,7 @@ def run_ours(args, w, dist, rank, world, local):
             e0.record(s_count)
             s_build.wait_event(e0)
             cnt_ms, calls = 0.0, 0
+            files_per_call = None
             for _ in range(K):
                 q = step()
                 # a step is one job: the next one starts when this one is done,
@@ -411,10 +416,11 @@ def run_ours(args, w, dist, rank, world, local):
         torch.cuda.synchronize()
         dist_barrier(dist, local)
         ms = e0.elapsed_time(e1) / K
-        return ms, launches, (cnt_ms / calls if calls else None), clk.summary()
+        files_per_call = nf * K / calls if calls else None
+        return ms, launches, (cnt_ms / calls if calls else None), files_per_call, clk.summary()
 
     K, W = args.steps, args.warmup
-    ms, launches, count_ms, clocks = timed(step_resident, K, W)
+    ms, launches, count_ms, files_per_call, clocks = timed(step_resident, K, W)
     ms = dist_max(dist, ms, local)
     if args.no_e2e:
         ms_e2e, launches_e2e, clocks_e2e = float("nan"), 0, None
@@ -512,11 +518,14 @@ def run_ours(args, w, dist, rank, world, local):
     peak, peak_kind = measured_peak()
     roof = None
     if count_ms:
-        achieved = ALGO_BYTES_PER_HALO_FILE * nh / (count_ms / 1e3) / 1e9
+        # one launch counts nh halos against files_per_call indexes
+        hf = nh * files_per_call
+        achieved = ALGO_BYTES_PER_HALO_FILE * hf / (count_ms / 1e3) / 1e9
         roof = {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
-                "frac": round(achieved / peak, 4), "traffic": profile_traffic(nh),
-                "kernel": "k_shell_count", "launch_ms": round(count_ms, 3),
-                "algorithmic_bytes_per_launch": ALGO_BYTES_PER_HALO_FILE * nh,
+                "frac": round(achieved / peak, 4), "traffic": profile_traffic(hf, files_per_call > 1),
+                "kernel": "k_shell_count_multi" if files_per_call > 1 else "k_shell_count",
+                "files_per_launch": round(files_per_call, 3), "launch_ms": round(count_ms, 3),
+                "algorithmic_bytes_per_launch": ALGO_BYTES_PER_HALO_FILE * hf,
                 "peak_kind": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else peak_kind}
     build_ms = statistics.median(bk)
     build_bytes = 24.0 * n + 4.0 * (ncells + 1)  # 12 B read + 12 B written per particle, 4 B per cell
@@ -544,6 +553,7 @@ def run_ours(args, w, dist, rank, world, local):
         "dtype": "f32", "data": "synthetic: reference generator streams (MT19937 seeds 1 and 2)",
         "config": {"workload": workload_name(w), "index": "grid (cell table, partition build)",
                    "build_kernels": "beside the counts" if args.overlap else "after the queued counts (copies overlap)",
+                   "count": "one fused pass over the step's files (sjcs_query_count_many)",
                    "parallelism": "replicas" if world > 1 else "single",
                    "l2": f"inputs larger than L2 ({nf} x {n * 12 / 1e9:.2f} GB particle arrays per step)"},
         "build_s_per_file": round(statistics.mean(bt) / 1e3, 5),

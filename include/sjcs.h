@@ -278,6 +278,16 @@ int sjcs_query_create_device(sjcs_ctx *ctx, const float *d_halo_xyz, size_t stri
  * multiRangeCountWithPriodicBoundArraySTR (include/objects/ArraySTR/MultiRangeCount.h:11)
  * or, without SJCS_QUERY_PERIODIC, of multiRangeCountArraySTR (:10). */
 int sjcs_query_count(sjcs_ctx *ctx, sjcs_query *q, const sjcs_index *idx);
+/* The counts of sjcs_query_count(ctx, q, idx[i]) for i = 0 .. k-1, added to
+ * the query's accumulators.  Runs of up to 4 grid indexes with the same cell
+ * grid (equal particle counts and radius hints give the same automatic grid),
+ * under the static schedule, are counted in one pass: each halo's rows are
+ * planned once and its counters flushed once for the whole run, and the
+ * indexes' row loads overlap each other's tests.  Any other index is counted
+ * on its own.  The reference's file loop (src/astr_rcount/main.c:676-826)
+ * counts one file at a time; this is the same sum over files with every
+ * file's index resident at once. */
+int sjcs_query_count_many(sjcs_ctx *ctx, sjcs_query *q, const sjcs_index *const *idx, int k);
 /* Block until the last sjcs_query_count queued on q has finished (builds
  * queued on the build stream keep running). */
 int sjcs_query_wait(sjcs_query *q);

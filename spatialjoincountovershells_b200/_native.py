@@ -126,6 +126,7 @@ _SIGS = {
     "sjcs_query_create": (_c.c_int, [_vp, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _pp]),
     "sjcs_query_create_device": (_c.c_int, [_vp, _vp, _c.c_size_t, _u64, _vp, _c.c_int, _c.c_int, _pp]),
     "sjcs_query_count": (_c.c_int, [_vp, _vp, _vp]),
+    "sjcs_query_count_many": (_c.c_int, [_vp, _vp, _vp, _c.c_int]),
     "sjcs_query_wait": (_c.c_int, [_vp]),
     "sjcs_index_build_file": (_c.c_int, [_vp, _c.c_char_p, _c.POINTER(sjcs_index_opts), _pp]),
     "sjcs_ctx_prepare_files": (_c.c_int, [_vp, _u64]),
@@ -536,6 +537,14 @@ class Query:
 
     def count(self, index: Index) -> "Query":
         _check(lib().sjcs_query_count(self.ctx._h, self._h, index._h))
+        return self
+
+    def count_many(self, indexes) -> "Query":
+        """The counts of count(i) for every index i, grid indexes of one cell
+        grid counted in one pass (up to 4 at a time)."""
+        indexes = list(indexes)
+        arr = (_vp * max(1, len(indexes)))(*[i._h for i in indexes])
+        _check(lib().sjcs_query_count_many(self.ctx._h, self._h, arr, len(indexes)))
         return self
 
     def wait(self) -> "Query":

@@ -1079,6 +1079,63 @@ int sjcs_query_count(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* idx) {
     return rc;
 }
 
+int sjcs_query_count_many(sjcs_ctx* ctx, sjcs_query* q, const sjcs_index* const* idx, int k) {
+    if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");
+    if (!valid_query(q) || q->ctx != ctx) return fail(SJCS_ERR_STATE, "query does not belong to this context");
+    if (k < 0 || (k > 0 && !idx)) return fail(SJCS_ERR_INVALID, "idx is NULL or k < 0");
+    for (int i = 0; i < k; ++i)
+        if (!valid_index(idx[i]) || idx[i]->ctx != ctx)
+            return fail(SJCS_ERR_STATE, "index %d does not belong to this context", i);
+    int rc = set_device(ctx);
+    if (rc) return rc;
+    // Fused: runs of up to kMaxFused grid indexes of one geometry under the
+    // static schedule whose counts fit the accumulators together; anything
+    // else is counted index by index.
+    for (int i = 0; i < k;) {
+        int j = i + 1;
+        const sjcs_index* a = idx[i];
+        bool fuse = a->kind == SJCS_INDEX_GRID;
+        if (fuse) {
+            std::lock_guard<std::mutex> lk(ctx->mu);
+            fuse = schedule_for(ctx, q, a).mode != SJCS_SCHED_QUEUE;
+        }
+        uint64_t add = count_call_bound(q->flags, q->r2max, a->n);
+        while (fuse && j < k && j - i < kMaxFusedIndexes) {
+            const sjcs_index* b = idx[j];
+            const uint64_t add_b = count_call_bound(q->flags, q->r2max, b->n);
+            if (b->kind != SJCS_INDEX_GRID || b->geom.ncells != a->geom.ncells || b->geom.G[0] != a->geom.G[0] ||
+                b->geom.G[1] != a->geom.G[1] || b->geom.G[2] != a->geom.G[2] || add + add_b > q->fold_limit)
+                break;
+            add += add_b;
+            ++j;
+        }
+        if (j - i == 1) {
+            rc = sjcs_query_count(ctx, q, a);
+            if (rc) return rc;
+            i = j;
+            continue;
+        }
+        std::lock_guard<std::mutex> lk(ctx->mu);
+        cudaStream_t s = ctx->s_count;
+        for (int t = i; t < j; ++t) SJCS_CUDA_TRY(cudaStreamWaitEvent(s, idx[t]->ev_ready, 0));
+        SJCS_CUDA_TRY(after_reads(q, s));
+        rc = fold_before_count(ctx, q, add, s);
+        if (rc) return rc;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        SJCS_CUDA_TRY(cudaEventCreate(&e0));
+        SJCS_CUDA_TRY(cudaEventCreate(&e1));
+        q->count_events.push_back(e0);
+        q->count_events.push_back(e1);
+        cudaEventRecord(e0, s);
+        rc = launch_shell_count_multi(ctx, q, idx + i, j - i, s);
+        cudaEventRecord(e1, s);
+        cudaEventRecord(q->ev_last, s);
+        if (rc) return rc;
+        i = j;
+    }
+    return SJCS_OK;
+}
+
 int sjcs_step_create(sjcs_ctx* ctx, sjcs_query* q, const float* host_xyz, uint64_t n, const sjcs_index_opts* opts,
                      sjcs_step** out) {
     if (!valid_ctx(ctx)) return fail(SJCS_ERR_STATE, "invalid context");

@@ -268,6 +268,11 @@ struct Schedule {
 };
 int launch_shell_count(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* idx, cudaStream_t s,
                        const Schedule* sc = nullptr);
+// k (1..kMaxFusedIndexes) grid indexes of one geometry counted in one
+// static-schedule pass: the counts of k launch_shell_count calls.
+constexpr int kMaxFusedIndexes = 4;
+int launch_shell_count_multi(sjcs_ctx* ctx, const sjcs_query* q, const sjcs_index* const* idx, int k,
+                             cudaStream_t s);
 
 // scan.cu: exclusive prefix sum of m u32 values, in place.  `partials`
 // (scan_partials_needed(m) u32) may be given; otherwise it is allocated.
