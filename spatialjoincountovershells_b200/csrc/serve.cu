@@ -125,11 +125,27 @@ int enqueue(sjcs_server* srv, Slot& sl) {
     if (rc) return rc;
     if (n) {
         std::lock_guard<std::mutex> lk(srv->ctx->mu);  // launch set-up and the tuned-schedule cache
-        for (const sjcs_index* ix : srv->idx) {
-            const Schedule sc = schedule_for(srv->ctx, &sl.q, ix);
-            rc = ix->kind == SJCS_INDEX_GRID ? launch_shell_count(srv->ctx, &sl.q, ix, s, &sc)
-                                             : launch_morton_count(srv->ctx, &sl.q, ix, s, &sc);
+        // grid indexes of one cell grid under the static schedule: one fused
+        // pass (each halo planned once for all of them)
+        const size_t k = srv->idx.size();
+        bool fuse = k >= 2 && k <= (size_t)kMaxFusedIndexes;
+        for (size_t i = 0; fuse && i < k; ++i) {
+            const sjcs_index* a = srv->idx[0];
+            const sjcs_index* b = srv->idx[i];
+            fuse = b->kind == SJCS_INDEX_GRID && b->geom.ncells == a->geom.ncells && b->geom.G[0] == a->geom.G[0] &&
+                   b->geom.G[1] == a->geom.G[1] && b->geom.G[2] == a->geom.G[2];
+        }
+        if (fuse) fuse = schedule_for(srv->ctx, &sl.q, srv->idx[0]).mode != SJCS_SCHED_QUEUE;
+        if (fuse) {
+            rc = launch_shell_count_multi(srv->ctx, &sl.q, srv->idx.data(), (int)k, s);
             if (rc) return rc;
+        } else {
+            for (const sjcs_index* ix : srv->idx) {
+                const Schedule sc = schedule_for(srv->ctx, &sl.q, ix);
+                rc = ix->kind == SJCS_INDEX_GRID ? launch_shell_count(srv->ctx, &sl.q, ix, s, &sc)
+                                                 : launch_morton_count(srv->ctx, &sl.q, ix, s, &sc);
+                if (rc) return rc;
+            }
         }
     }
     const size_t cnt = (size_t)n * (size_t)nrads;
