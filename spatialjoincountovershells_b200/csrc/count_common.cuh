@@ -123,8 +123,7 @@ __device__ __forceinline__ void test_candidate(const CountParams& p, const Image
 // Scan the lanes' row lengths and test every candidate of those rows,
 // two windows of 32 candidates per iteration so two loads are in flight.
 template <int BIN, bool BIG>
-__device__ __forceinline__ void run_rows(const CountParams& p, const float4* __restrict__ pts, const Image& im,
-                                         uint32_t start, uint32_t end,
+__device__ __forceinline__ void run_rows(const CountParams& p, const Image& im, uint32_t start, uint32_t end,
                                          uint32_t* __restrict__ sink, const float* __restrict__ tab,
                                          const uint32_t* __restrict__ lut, int lane) {
     const uint32_t len = end - start;
@@ -150,8 +149,8 @@ __device__ __forceinline__ void run_rows(const CountParams& p, const float4* __r
         const uint32_t o0 = __shfl_sync(0xffffffffu, off, r0);
         const uint32_t o1 = __shfl_sync(0xffffffffu, off, r1);
         const bool l0 = t0 < total, l1 = t1 < total;
-        const float4 p0 = l0 ? __ldg(pts + (t0 + o0)) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 p1 = l1 ? __ldg(pts + (t1 + o1)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 p0 = l0 ? __ldg(p.pts + (t0 + o0)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 p1 = l1 ? __ldg(p.pts + (t1 + o1)) : make_float4(0.f, 0.f, 0.f, 0.f);
         test_candidate<BIN, BIG>(p, im, p0, l0, sink, tab, lut);
         test_candidate<BIN, BIG>(p, im, p1, l1, sink, tab, lut);
     }
@@ -162,8 +161,7 @@ __device__ __forceinline__ void run_rows(const CountParams& p, const float4* __r
 // flattened candidate sequence, so nparts warps sharing a halo split every
 // row set evenly and together test each candidate once.
 template <int BIN, bool BIG>
-__device__ __forceinline__ void run_rows_part(const CountParams& p, const float4* __restrict__ pts, const Image& im,
-                                              uint32_t start, uint32_t end,
+__device__ __forceinline__ void run_rows_part(const CountParams& p, const Image& im, uint32_t start, uint32_t end,
                                               uint32_t* __restrict__ sink, const float* __restrict__ tab,
                                               const uint32_t* __restrict__ lut, int lane, uint32_t part,
                                               uint32_t nparts) {
@@ -191,8 +189,8 @@ __device__ __forceinline__ void run_rows_part(const CountParams& p, const float4
         const uint32_t o0 = __shfl_sync(0xffffffffu, off, r0);
         const uint32_t o1 = __shfl_sync(0xffffffffu, off, r1);
         const bool l0 = t0 < te, l1 = t1 < te;
-        const float4 p0 = l0 ? __ldg(pts + (t0 + o0)) : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 p1 = l1 ? __ldg(pts + (t1 + o1)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 p0 = l0 ? __ldg(p.pts + (t0 + o0)) : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 p1 = l1 ? __ldg(p.pts + (t1 + o1)) : make_float4(0.f, 0.f, 0.f, 0.f);
         test_candidate<BIN, BIG>(p, im, p0, l0, sink, tab, lut);
         test_candidate<BIN, BIG>(p, im, p1, l1, sink, tab, lut);
     }

@@ -64,8 +64,8 @@ template <int BIN, bool BIG>
 __device__ __forceinline__ void run_ranges(const CountParams& p, const Image& im, uint32_t s0, uint32_t s1,
                                            uint32_t* __restrict__ sink, const float* __restrict__ tab,
                                            const uint32_t* __restrict__ lut, int lane, uint32_t part, uint32_t nparts) {
-    if (nparts > 1) run_rows_part<BIN, BIG>(p, p.pts, im, s0, s1, sink, tab, lut, lane, part, nparts);
-    else run_rows<BIN, BIG>(p, p.pts, im, s0, s1, sink, tab, lut, lane);
+    if (nparts > 1) run_rows_part<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane, part, nparts);
+    else run_rows<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane);
 }
 
 template <int LOOK, int BIN, bool BIG>

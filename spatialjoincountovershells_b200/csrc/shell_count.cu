@@ -72,8 +72,7 @@ __device__ __forceinline__ void row_yz(const Image& im, uint32_t r, int* yy, int
 // sphere and fetch the row's first and one-past-last slots.  Returns the
 // slot range through *start / *end (empty: start == end).  gy_l / gz_l are
 // the lane-distributed gap tables of the image (valid when ny, nz <= 32).
-__device__ __forceinline__ void row_issue(const CountParams& p, const uint32_t* __restrict__ cs, const Image& im,
-                                          uint32_t rb, int lane,
+__device__ __forceinline__ void row_issue(const CountParams& p, const Image& im, uint32_t rb, int lane,
                                           float gy_l, float gz_l, uint32_t* start, uint32_t* end) {
     const uint32_t r = rb + (uint32_t)lane;
     int yy = 0, zz = 0;
@@ -104,8 +103,8 @@ __device__ __forceinline__ void row_issue(const CountParams& p, const uint32_t* 
     uint32_t s0 = 0, s1 = 0;
     if (live && xa <= xb) {
         const uint64_t rowcell = ((uint64_t)zz * (uint64_t)p.g.G[1] + (uint64_t)yy) * (uint64_t)p.g.G[0];
-        s0 = __ldg(cs + rowcell + xa);
-        s1 = __ldg(cs + rowcell + xb + 1);
+        s0 = __ldg(p.cs + rowcell + xa);
+        s1 = __ldg(p.cs + rowcell + xb + 1);
     }
     *start = s0;
     *end = s1;
@@ -123,24 +122,22 @@ __device__ __forceinline__ void gap_tables(const CountParams& p, const Image& im
 
 // Every row chunk of an image from chunk `first_chunk` on, synchronously.
 template <int BIN, bool BIG>
-__device__ __forceinline__ void count_image(const CountParams& p, const float4* __restrict__ pts,
-                                            const uint32_t* __restrict__ cs, const Image& im, uint32_t first_chunk,
+__device__ __forceinline__ void count_image(const CountParams& p, const Image& im, uint32_t first_chunk,
                                             uint32_t* __restrict__ sink, const float* __restrict__ tab,
                                             const uint32_t* __restrict__ lut, int lane) {
     float gy, gz;
     gap_tables(p, im, lane, &gy, &gz);
     for (uint32_t rb = first_chunk * 32u; rb < im.nrows; rb += 32u) {
         uint32_t s0, s1;
-        row_issue(p, cs, im, rb, lane, gy, gz, &s0, &s1);
-        run_rows<BIN, BIG>(p, pts, im, s0, s1, sink, tab, lut, lane);
+        row_issue(p, im, rb, lane, gy, gz, &s0, &s1);
+        run_rows<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane);
     }
 }
 
 // Piece `part` of `nparts` of every row chunk of an image (heavy halos
 // shared by several warps).
 template <int BIN, bool BIG>
-__device__ __forceinline__ void count_image_part(const CountParams& p, const float4* __restrict__ pts,
-                                                 const uint32_t* __restrict__ cs, const Image& im,
+__device__ __forceinline__ void count_image_part(const CountParams& p, const Image& im,
                                                  uint32_t* __restrict__ sink, const float* __restrict__ tab,
                                                  const uint32_t* __restrict__ lut, int lane, uint32_t part,
                                                  uint32_t nparts) {
@@ -148,8 +145,8 @@ __device__ __forceinline__ void count_image_part(const CountParams& p, const flo
     gap_tables(p, im, lane, &gy, &gz);
     for (uint32_t rb = 0; rb < im.nrows; rb += 32u) {
         uint32_t s0, s1;
-        row_issue(p, cs, im, rb, lane, gy, gz, &s0, &s1);
-        run_rows_part<BIN, BIG>(p, pts, im, s0, s1, sink, tab, lut, lane, part, nparts);
+        row_issue(p, im, rb, lane, gy, gz, &s0, &s1);
+        run_rows_part<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane, part, nparts);
     }
 }
 
@@ -157,8 +154,7 @@ __device__ __forceinline__ void count_image_part(const CountParams& p, const flo
 // the flagged axes (MultiRangeCount.c:31-71).  nparts > 1: this warp's piece
 // of each image only.
 template <int BIN, bool BIG>
-__device__ __forceinline__ void count_shifted_images(const CountParams& p, const float4* __restrict__ pts,
-                                                     const uint32_t* __restrict__ cs, const float4 c,
+__device__ __forceinline__ void count_shifted_images(const CountParams& p, const float4 c,
                                                      uint32_t* __restrict__ sink, const float* __restrict__ tab,
                                                      const uint32_t* __restrict__ lut, int lane,
                                                      uint32_t part = 0, uint32_t nparts = 1) {
@@ -175,8 +171,8 @@ __device__ __forceinline__ void count_shifted_images(const CountParams& p, const
     const float sz = (loz < kBoxLow) ? __fadd_rn(c.z, kBoxUpp) : __fsub_rn(c.z, kBoxUpp);
     for (unsigned S = F; S != 0; S = (S - 1u) & F) {
         const Image im = make_image(p, (S & 1u) ? sx : c.x, (S & 2u) ? sy : c.y, (S & 4u) ? sz : c.z);
-        if (nparts > 1) count_image_part<BIN, BIG>(p, pts, cs, im, sink, tab, lut, lane, part, nparts);
-        else count_image<BIN, BIG>(p, pts, cs, im, 0, sink, tab, lut, lane);
+        if (nparts > 1) count_image_part<BIN, BIG>(p, im, sink, tab, lut, lane, part, nparts);
+        else count_image<BIN, BIG>(p, im, 0, sink, tab, lut, lane);
     }
 }
 
@@ -249,14 +245,13 @@ __device__ __forceinline__ void plan_halo(const CountParams& p, float4 c, bool v
 }
 
 // Lane r fetches the slot range of row r of planned halo k.
-__device__ __forceinline__ void fetch_rows(const uint32_t* __restrict__ cs, const WarpPlans* wp, uint32_t k,
-                                           uint32_t nrows,
+__device__ __forceinline__ void fetch_rows(const CountParams& p, const WarpPlans* wp, uint32_t k, uint32_t nrows,
                                            int lane, uint32_t* s0, uint32_t* s1) {
     uint32_t a = 0, b = 0;
     if ((uint32_t)lane < nrows) {
         const uint32_t c0 = wp->row_cell[k][lane];
-        a = __ldg(cs + c0);
-        b = __ldg(cs + c0 + wp->row_len[k][lane]);
+        a = __ldg(p.cs + c0);
+        b = __ldg(p.cs + c0 + wp->row_len[k][lane]);
     }
     *s0 = a;
     *s1 = b;
@@ -294,7 +289,7 @@ __device__ __forceinline__ void count_batch(const CountParams& p, WarpPlans* wp,
     uint32_t s0, s1;
     {
         const uint32_t n0 = wp->plan[0].nrows;
-        fetch_rows(p.cs, wp, 0, n0 == kSlowPlan ? 0u : n0, lane, &s0, &s1);
+        fetch_rows(p, wp, 0, n0 == kSlowPlan ? 0u : n0, lane, &s0, &s1);
     }
     for (uint32_t k = 0; k < nb; ++k) {
         const HaloPlan pl = wp->plan[k];
@@ -302,7 +297,7 @@ __device__ __forceinline__ void count_batch(const CountParams& p, WarpPlans* wp,
         uint32_t t0 = 0, t1 = 0;
         if (k + 1 < nb) {
             const uint32_t nn = wp->plan[k + 1].nrows;
-            fetch_rows(p.cs, wp, k + 1, nn == kSlowPlan ? 0u : nn, lane, &t0, &t1);
+            fetch_rows(p, wp, k + 1, nn == kSlowPlan ? 0u : nn, lane, &t0, &t1);
         }
         uint32_t* row = p.counts + (uint64_t)pl.row * (uint64_t)p.nrads;
         uint32_t* sink = BIG ? row : wcnt;
@@ -317,12 +312,11 @@ __device__ __forceinline__ void count_batch(const CountParams& p, WarpPlans* wp,
         im.loz = __fsub_rn(pl.cz, p.half);
         im.hiz = __fadd_rn(pl.cz, p.half);
         if (pl.nrows == kSlowPlan) {
-            count_image<BIN, BIG>(p, p.pts, p.cs, make_image(p, pl.cx, pl.cy, pl.cz), 0, sink, tab, lut, lane);
+            count_image<BIN, BIG>(p, make_image(p, pl.cx, pl.cy, pl.cz), 0, sink, tab, lut, lane);
         } else {
-            run_rows<BIN, BIG>(p, p.pts, im, s0, s1, sink, tab, lut, lane);
+            run_rows<BIN, BIG>(p, im, s0, s1, sink, tab, lut, lane);
         }
-        if (pl.flags)
-            count_shifted_images<BIN, BIG>(p, p.pts, p.cs, make_float4(pl.cx, pl.cy, pl.cz, 0.f), sink, tab, lut, lane);
+        if (pl.flags) count_shifted_images<BIN, BIG>(p, make_float4(pl.cx, pl.cy, pl.cz, 0.f), sink, tab, lut, lane);
         if (!BIG) flush_counts(p, wcnt, row, lane);
         s0 = t0;
         s1 = t1;
@@ -330,26 +324,28 @@ __device__ __forceinline__ void count_batch(const CountParams& p, WarpPlans* wp,
     __syncwarp();  // the batch's plans are read before the next batch overwrites them
 }
 
-// count_batch over several indexes of one grid (p.nidx of them): a halo is planned once, and its rows are fetched from every
-// index in turn -- the next (halo, index) pair's row loads in flight during
-// the current pair's tests -- before its counters are flushed once.
+// count_batch over several indexes of one grid (p.nidx of them): a halo is
+// planned once, and its rows are fetched from every index in turn -- the
+// next (halo, index) pair's row loads in flight during the current pair's
+// tests -- before its counters are flushed once.  Each index is counted
+// through a copy of the parameters that points at it, so the row and
+// candidate code is the single-index code.
 template <int BIN, bool BIG>
-__device__ __forceinline__ void count_batch_multi(const CountParams& p, WarpPlans* wp, uint32_t nb,
-                                                  float4 c_lane, uint32_t* __restrict__ wcnt,
-                                                  const float* __restrict__ tab, const uint32_t* __restrict__ lut,
-                                                  int lane) {
+__device__ __forceinline__ void count_batch_multi(const CountParams& p, WarpPlans* wp, uint32_t nb, float4 c_lane,
+                                                  uint32_t* __restrict__ wcnt, const float* __restrict__ tab,
+                                                  const uint32_t* __restrict__ lut, int lane) {
     {
         const bool valid = (uint32_t)lane < nb;
         plan_halo(p, c_lane, valid, &wp->plan[lane], wp->row_cell[lane], wp->row_len[lane]);
     }
     __syncwarp();
     const int nf = p.nidx;
-    const float4* const* mpts = p.mpts;
-    const uint32_t* const* mcs = p.mcs;
     uint32_t s0, s1;
     {
+        CountParams p0 = p;
+        p0.cs = p.mcs[0];
         const uint32_t n0 = wp->plan[0].nrows;
-        fetch_rows(mcs[0], wp, 0, n0 == kSlowPlan ? 0u : n0, lane, &s0, &s1);
+        fetch_rows(p0, wp, 0, n0 == kSlowPlan ? 0u : n0, lane, &s0, &s1);
     }
     for (uint32_t k = 0; k < nb; ++k) {
         for (int f = 0; f < nf; ++f) {
@@ -357,16 +353,20 @@ __device__ __forceinline__ void count_batch_multi(const CountParams& p, WarpPlan
             const uint32_t kn = last ? k + 1 : k;
             uint32_t t0 = 0, t1 = 0;
             if (kn < nb) {
+                CountParams pn = p;
+                pn.cs = p.mcs[last ? 0 : f + 1];
                 const uint32_t nn = wp->plan[kn].nrows;
-                fetch_rows(mcs[last ? 0 : f + 1], wp, kn, nn == kSlowPlan ? 0u : nn, lane, &t0, &t1);
+                fetch_rows(pn, wp, kn, nn == kSlowPlan ? 0u : nn, lane, &t0, &t1);
             }
+            CountParams pf = p;
+            pf.pts = p.mpts[f];
+            pf.cs = p.mcs[f];
             // the plan and box are read again per index: fewer registers live
             // across the index loop
             const HaloPlan pl = wp->plan[k];
             uint32_t* sink = BIG ? p.counts + (uint64_t)pl.row * (uint64_t)p.nrads : wcnt;
-            const float4* pts = mpts[f];
             if (pl.nrows == kSlowPlan) {
-                count_image<BIN, BIG>(p, pts, mcs[f], make_image(p, pl.cx, pl.cy, pl.cz), 0, sink, tab, lut, lane);
+                count_image<BIN, BIG>(pf, make_image(pf, pl.cx, pl.cy, pl.cz), 0, sink, tab, lut, lane);
             } else {
                 Image im;
                 im.cx = pl.cx;
@@ -378,11 +378,9 @@ __device__ __forceinline__ void count_batch_multi(const CountParams& p, WarpPlan
                 im.hiy = __fadd_rn(pl.cy, p.half);
                 im.loz = __fsub_rn(pl.cz, p.half);
                 im.hiz = __fadd_rn(pl.cz, p.half);
-                run_rows<BIN, BIG>(p, pts, im, s0, s1, sink, tab, lut, lane);
+                run_rows<BIN, BIG>(pf, im, s0, s1, sink, tab, lut, lane);
             }
-            if (pl.flags)
-                count_shifted_images<BIN, BIG>(p, pts, mcs[f], make_float4(pl.cx, pl.cy, pl.cz, 0.f), sink, tab, lut,
-                                               lane);
+            if (pl.flags) count_shifted_images<BIN, BIG>(pf, make_float4(pl.cx, pl.cy, pl.cz, 0.f), sink, tab, lut, lane);
             s0 = t0;
             s1 = t1;
         }
@@ -537,10 +535,9 @@ __global__ void __launch_bounds__(CT_THREADS, 8) k_shell_count_queue(CountParams
             uint32_t* row = p.counts + (uint64_t)__float_as_uint(c.w) * (uint64_t)p.nrads;
             uint32_t* sink = BIG ? row : v.wcnt;
             const Image im = make_image(p, c.x, c.y, c.z);
-            if (bp.pieces > 1) count_image_part<BIN, BIG>(p, p.pts, p.cs, im, sink, v.tab, v.lut, lane, part, bp.pieces);
-            else count_image<BIN, BIG>(p, p.pts, p.cs, im, 0, sink, v.tab, v.lut, lane);
-            if (p.periodic)
-                count_shifted_images<BIN, BIG>(p, p.pts, p.cs, c, sink, v.tab, v.lut, lane, part, bp.pieces);
+            if (bp.pieces > 1) count_image_part<BIN, BIG>(p, im, sink, v.tab, v.lut, lane, part, bp.pieces);
+            else count_image<BIN, BIG>(p, im, 0, sink, v.tab, v.lut, lane);
+            if (p.periodic) count_shifted_images<BIN, BIG>(p, c, sink, v.tab, v.lut, lane, part, bp.pieces);
             if (!BIG) flush_counts(p, v.wcnt, row, lane);
         } else {
             const uint32_t first = r * bp.per;
