@@ -261,6 +261,10 @@ int sjcs_index_destroy(sjcs_index *idx);
  * src/astr_rcount/main.c:644-649); any table is accepted -- a non-decreasing,
  * finite one takes the fast binning path, anything else the reference's
  * first-match scan.  flags: SJCS_QUERY_PERIODIC or SJCS_QUERY_NONPERIODIC.
+ * The halos go up on the context's upload stream (beside counts already
+ * queued); halos in page-locked memory are read after the call returns and
+ * must stay unchanged until the query's first count has finished
+ * (sjcs_query_wait), pageable ones are copied before it returns.
  * Replaces constructMultiRangeCountContext + the per-row set-up in threadJoin
  * (src/objects/RTree/MultiRangeCountContext.c:8-25, src/astr_rcount/main.c:816-821). */
 int sjcs_query_create(sjcs_ctx *ctx, const float *halo_xyz, size_t stride_bytes,

@@ -1013,20 +1013,28 @@ int sjcs_query_create(sjcs_ctx* ctx, const float* halo_xyz, size_t stride_bytes,
     std::lock_guard<std::mutex> lk(ctx->mu);
     sjcs_query* q = new_query(ctx);
     if (!q) return fail(SJCS_ERR_NOMEM, "out of host memory");
-    cudaStream_t s = ctx->s_count;
-    StreamScratch scr(s);
+    cudaStream_t s = ctx->s_count, u = ctx->s_h2d;
     float* d_raw = nullptr;
     // The last halo needs only its 12 coordinate bytes, not a whole stride.
     const size_t bytes = nhalos ? (size_t)(nhalos - 1) * stride_bytes + 3 * sizeof(float) : 0;
     if (nhalos) {
-        cudaError_t e = scr.alloc(&d_raw, bytes);
-        if (e == cudaSuccess) e = cudaMemcpyAsync(d_raw, halo_xyz, bytes, cudaMemcpyHostToDevice, s);
+        // on the upload stream, so the copy overlaps counts already queued on
+        // the count stream; the count stream waits for it
+        cudaEvent_t ev = nullptr;
+        cudaError_t e = cudaMallocAsync(&d_raw, bytes, u);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(d_raw, halo_xyz, bytes, cudaMemcpyHostToDevice, u);
+        if (e == cudaSuccess) e = cudaEventCreateWithFlags(&ev, cudaEventDisableTiming);
+        if (e == cudaSuccess) e = cudaEventRecord(ev, u);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s, ev, 0);
+        if (ev) cudaEventDestroy(ev);
         if (e != cudaSuccess) {
+            if (d_raw) cudaFreeAsync(d_raw, u);
             free_query(q);
             return fail(SJCS_ERR_CUDA, "halo upload failed: %s", cudaGetErrorString(e));
         }
     }
-    rc = query_prepare(ctx, d_raw, stride_bytes, nhalos, r2, nrads, flags, q, ctx->s_count);
+    rc = query_prepare(ctx, d_raw, stride_bytes, nhalos, r2, nrads, flags, q, s);
+    if (d_raw) cudaFreeAsync(d_raw, s);  // after the halo sort that reads it
     if (rc) {
         free_query(q);
         return rc;
