@@ -185,9 +185,11 @@ __device__ __forceinline__ uint32_t pb_block_scan(uint32_t v, uint32_t* ws, uint
 __device__ __forceinline__ uint32_t pb_key(const float4& r) { return __float_as_uint(r.w); }
 
 // top_hist[cell >> shift] += 1 for every particle (at most PB_THREADS bins,
-// counted in shared memory first).  A block stages its 4096 particles' x,y,z
-// in shared memory with coalesced 16-byte copies (cp.async when the array is
-// 16-byte aligned) and takes the keys from there.
+// counted in shared memory first).  Block b takes tiles PB_TOP_TILES*b ..
+// (one reduction per bin for all of them); each tile's x,y,z are staged in
+// shared memory with coalesced 16-byte copies (cp.async when the array is
+// 16-byte aligned) and the keys taken from there.
+constexpr uint32_t PB_TOP_TILES = 4;
 __global__ void __launch_bounds__(PB_THREADS)
 k_pb_top_hist(const float* __restrict__ xyz, int aligned, uint64_t n, GridGeom g, int shift,
               uint32_t* __restrict__ top_hist) {
@@ -196,24 +198,28 @@ k_pb_top_hist(const float* __restrict__ xyz, int aligned, uint64_t n, GridGeom g
     float* sx = reinterpret_cast<float*>(stage4);
     const int tid = threadIdx.x;
     sh[tid] = 0u;
-    const uint64_t start = (uint64_t)blockIdx.x * PB_TILE;
-    const uint64_t rem = n - start;
-    const uint32_t len = rem < PB_TILE ? (uint32_t)rem : PB_TILE;
-    const float* src = xyz + 3 * start;
-    const uint32_t words = 3u * len;
-    uint32_t w0 = 0;
-    if (aligned) {
-        const uint32_t chunks = words >> 2;
-        for (uint32_t c = (uint32_t)tid; c < chunks; c += PB_THREADS) cp_async16(sx + 4 * c, src + 4 * c);
-        w0 = chunks * 4u;
-    }
-    for (uint32_t w = w0 + (uint32_t)tid; w < words; w += PB_THREADS) sx[w] = src[w];
-    cp_async_wait_all();
-    __syncthreads();
+    for (uint32_t t = 0; t < PB_TOP_TILES; ++t) {
+        const uint64_t start = ((uint64_t)blockIdx.x * PB_TOP_TILES + t) * PB_TILE;
+        if (start >= n) break;  // uniform across the block
+        const uint64_t rem = n - start;
+        const uint32_t len = rem < PB_TILE ? (uint32_t)rem : PB_TILE;
+        const float* src = xyz + 3 * start;
+        const uint32_t words = 3u * len;
+        uint32_t w0 = 0;
+        __syncthreads();  // the previous tile's staged words have been read
+        if (aligned) {
+            const uint32_t chunks = words >> 2;
+            for (uint32_t c = (uint32_t)tid; c < chunks; c += PB_THREADS) cp_async16(sx + 4 * c, src + 4 * c);
+            w0 = chunks * 4u;
+        }
+        for (uint32_t w = w0 + (uint32_t)tid; w < words; w += PB_THREADS) sx[w] = src[w];
+        cp_async_wait_all();
+        __syncthreads();
 #pragma unroll
-    for (int i = 0; i < PB_ITEMS; ++i) {
-        const uint32_t loc = (uint32_t)i * PB_THREADS + (uint32_t)tid;
-        if (loc < len) atomicAdd(&sh[cell_key(g, sx[3 * loc], sx[3 * loc + 1], sx[3 * loc + 2]) >> shift], 1u);
+        for (int i = 0; i < PB_ITEMS; ++i) {
+            const uint32_t loc = (uint32_t)i * PB_THREADS + (uint32_t)tid;
+            if (loc < len) atomicAdd(&sh[cell_key(g, sx[3 * loc], sx[3 * loc + 1], sx[3 * loc + 2]) >> shift], 1u);
+        }
     }
     __syncthreads();
     const uint32_t c = sh[tid];
@@ -540,7 +546,8 @@ int build_grid_partitioned(const float* d_xyz, uint64_t n, const GridGeom& g, fl
     SJCS_CUDA_TRY(cudaFuncSetAttribute(k_pb_top_hist, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                        (int)PB_STAGE_SMEM));
     SJCS_CUDA_TRY(cudaMemsetAsync(top, 0, ((uint64_t)ntop + 1) * sizeof(uint32_t), s));
-    k_pb_top_hist<<<(unsigned)ntiles_in, PB_THREADS, PB_STAGE_SMEM, s>>>(d_xyz, aligned, n, g, top_shift, top);
+    k_pb_top_hist<<<(unsigned)((ntiles_in + PB_TOP_TILES - 1) / PB_TOP_TILES), PB_THREADS, PB_STAGE_SMEM, s>>>(
+        d_xyz, aligned, n, g, top_shift, top);
     SJCS_LAUNCH_CHECK();
     int rc = exclusive_scan_u32(top, (uint64_t)ntop + 1, s);
     if (rc) return rc;
