@@ -125,3 +125,44 @@ def test_fused_other_kernel_variants(kind, ctx):
     q.destroy()
     want = sum(oracle.count(f, h, r2, periodic=periodic) for f in files)
     assert np.array_equal(got, want)
+
+
+def test_fresh_query_reads_zeros_and_fused_passes_add(six_files, ctx):
+    """Every read of a new query before a count gives zeros (host uint64,
+    host uint32 and the device pointer), and fused passes add up and
+    restart after a reset."""
+    import torch
+    files, h, r2, per_file = six_files
+    q = ctx.query(h, r2)
+    assert not q.read_counts().any()
+    buf = nat.PinnedBuffer((len(h), len(r2)), np.uint32)
+    buf.array[:] = 7
+    q.read_counts32_async(buf.array)
+    q.wait_read()
+    assert not buf.array.any()
+    q.destroy()
+    q = ctx.query(h, r2)
+    m = len(h) * len(r2)
+
+    class _U32:  # the accumulators as a CUDA array for torch to copy
+        __cuda_array_interface__ = {"shape": (m,), "typestr": "<i4", "data": (q.device_counts_ptr, False),
+                                    "version": 3}
+
+    dev = torch.as_tensor(_U32(), device="cuda").clone()
+    torch.cuda.synchronize()
+    assert not dev.any()
+    q.destroy()
+    q = ctx.query(h, r2)
+    q.set_schedule(nat.SCHED_STATIC)
+    idx = [ctx.build_index(f, radius_hint=12.0) for f in files[:3]]
+    q.count_many(idx)
+    assert np.array_equal(q.read_counts(), sum(per_file[:3]))
+    q.count_many(idx)
+    assert np.array_equal(q.read_counts(), 2 * sum(per_file[:3]))
+    q.reset()
+    q.count_many(idx)
+    assert np.array_equal(q.read_counts(), sum(per_file[:3]))
+    for i in idx:
+        i.destroy()
+    q.destroy()
+    buf.free()
