@@ -13,7 +13,7 @@ enum BinMode { BIN_LUT = 0, BIN_BSEARCH = 1, BIN_FIRST_MATCH = 2 };
 constexpr int kMaxFused = kMaxFusedIndexes;  // indexes counted in one pass by k_shell_count_multi
 
 struct CountParams {
-    const float4* __restrict__ pts;  // sorted particles (x, y, z, unused)
+    const float4* __restrict__ pts;  // particles grouped by cell (x, y, z; .w not read)
     const uint32_t* __restrict__ cs;
     GridGeom g;
     float h[3];                      // cell edge per axis, 1000 / G

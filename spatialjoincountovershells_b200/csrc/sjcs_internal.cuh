@@ -1,9 +1,10 @@
 // Internal declarations shared by the CUDA translation units of libsjcs.so.
 //
 // Data layout in HBM (one particle file = one index):
-//   pts[n]                float4 (x, y, z, unused), particles sorted by cell
-//                         key, so a warp reading 32 consecutive candidates
-//                         issues one coalesced 128-bit load per lane
+//   pts[n]                float4 (x, y, z, cell key bits; the LSD build leaves 0),
+//                         particles grouped by cell in cell order, so a warp
+//                         reading 32 consecutive candidates issues one
+//                         coalesced 128-bit load per lane
 //   cell_start[ncells+1]  u32, first sorted slot of every cell; cells are
 //                         numbered x-fastest ((cz*Gy + cy)*Gx + cx), so one
 //                         (cy, cz) row of cells is one contiguous slot range.
